@@ -1,0 +1,351 @@
+"""Exact-BC TEPS benchmark of the B200 engine (one JSON line on rank 0).
+
+Workload (N=1): R-MAT scale 20, edge factor 16, (a,b,c,d) = (0.57,0.19,0.19,
+0.05), seed 2, plus pendant trees on 10% of the vertices (Geometric sizes,
+mean 4); 4096 sources drawn uniformly without replacement with seed 2;
+degree-1 pruning on; FP64 delta/bc, uint64 sigma.  Seeded synthetic input:
+no public dataset is involved.
+
+A step = one exact-BC pass over the step's sources (one kernel launch of the
+engine), preceded (untimed) by a reset of the bc accumulator and an L2 flush
+(a 512 MiB device write, larger than the 126 MB L2).  With N ranks (one per
+GPU, torchrun) every rank takes its own block of 4096 sources (weak scaling)
+and the step ends with an NCCL all-reduce of the FP64 bc vector.
+
+  value  TEPS = sum over all ranks' sources of the undirected edge count of
+         the source's component / max-over-ranks device time (CUDA events on
+         the launching stream), graph and sources resident in HBM.
+  e2e    the same metric through the C ABI with host buffers: per step
+         bcg_graph_create (pinned host CSR -> device, pruning, tiles),
+         bcg_run (host source list), [all-reduce], bcg_get_bc (device -> host).
+  roofline  algorithmic bytes of the sweep kernel = sum over sources of
+         16*m_comp + 56*n_comp + 8 (int32 ids, uint64 sigma, FP64 delta/bc),
+         divided by its CUDA-event time; peak = MEASURED_PEAKS.json hbm_gbs.
+  cpu_baseline  the oracle (CPU Brandes restatement, all host threads) on a
+         bounded sample of the same workload's sources, rank 0 at N=1.
+--impl reference: the reference program has no CPU Brandes; its path is timed
+through the oracle port on the host cores (all threads), each step a bounded
+sample of the same sources.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "ck-bc_b200"))
+
+WORKLOAD = "rmat20_ef16_pendant10_4096src"
+SPEC = "rmat:scale=20,ef=16,a=0.57,b=0.19,c=0.19,seed=2,pendant_frac=0.1,pendant_mean=4"
+SRC_SEED = 2
+NSRC = 4096
+METRIC = "exact-BC TEPS (sources*edges/s)"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        busy = [s for s in sm if mx and s > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(busy) if busy else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_per_source():
+    """DRAM bytes per source of the sweep kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "sweep_traffic.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["dram_bytes_per_source"]), d.get("note", "")
+    except Exception:
+        return None, ""
+
+
+def cpu_baseline(offs, adj, sources, budget_s=15.0):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle
+
+    nt = oracle.max_threads()
+    done = 0
+    edges = 0
+    t0 = time.perf_counter()
+    chunk = max(nt, 1)
+    while done < len(sources) and time.perf_counter() - t0 < budget_s:
+        s = sources[done:done + chunk]
+        _, st = oracle.bc(offs, adj, s, nthreads=nt)
+        edges += st["teps_edges"]
+        done += len(s)
+    el = time.perf_counter() - t0
+    return {"value": edges / el if el > 0 else None, "unit": "TEPS", "cores": nt, "kind": "port",
+            "sample": f"first {done} of the {len(sources)} workload sources, oracle/brandes.c FP64 Brandes, "
+                      f"{nt} OpenMP threads, {el:.1f} s"}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference path's CPU restatement, all host threads."""
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import bcg
+    import oracle
+
+    offs, adj = bcg.generate(SPEC)
+    n = len(offs) - 1
+    srcs = bcg.sample_sources(n, NSRC, SRC_SEED)
+    nt = oracle.max_threads()
+    per_step = max(nt, 1)
+    times, edges = [], []
+    pos = 0
+    for i in range(args.warmup + args.steps):
+        s = srcs[pos:pos + per_step]
+        pos = (pos + per_step) % (len(srcs) - per_step)
+        t0 = time.perf_counter()
+        _, st = oracle.bc(offs, adj, s, nthreads=nt)
+        el = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(el)
+            edges.append(st["teps_edges"])
+    tot_t = sum(times)
+    val = sum(edges) / tot_t if tot_t > 0 else None
+    out = {"metric": METRIC, "value": val, "unit": "TEPS", "impl": "reference", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / max(1, len(times)),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": WORKLOAD, "graph": SPEC, "sources": NSRC, "source_seed": SRC_SEED,
+                      "sample_per_step": per_step},
+           "cpu_baseline": {"value": val, "unit": "TEPS", "cores": nt, "kind": "port",
+                            "sample": f"{per_step} sources per step of the workload's 4096, oracle/brandes.c "
+                                      f"(the reference has no CPU Brandes), {nt} OpenMP threads"},
+           "e2e": {"value": val, "unit": "TEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="bcg", choices=["bcg", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=0, help="e2e steps (default: min(steps, 3))")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sources", type=int, default=NSRC, help="sources per GPU (profiling runs use fewer)")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import numpy as np
+    import torch
+
+    import bcg
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    t_gen = time.perf_counter()
+    offs, adj = bcg.generate(SPEC)
+    n = len(offs) - 1
+    ns = args.sources
+    all_src = bcg.sample_sources(n, ns * world, SRC_SEED)
+    srcs = np.ascontiguousarray(all_src[rank * ns:(rank + 1) * ns])
+    log(f"[rank {rank}] graph n={n} nnz={len(adj)} generated in {time.perf_counter() - t_gen:.1f}s")
+
+    g = bcg.Graph(offs, adj, bcg.PRUNE_DEGREE1)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    bc_t = torch.as_tensor(bcg.DeviceArray(g.bc_device_ptr(), n), device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def one_step():
+        g.reset()
+        flush.zero_()
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        st = g.run(srcs)
+        if dist is not None:
+            dist.all_reduce(bc_t)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1), st
+
+    for _ in range(args.warmup):
+        one_step()
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    step_ms, kern_ms, edges, cverts, ran = [], [], 0, 0, 0
+    for _ in range(args.steps):
+        ms, st = one_step()
+        step_ms.append(ms)
+        kern_ms.append(st.kernel_ms)
+        edges += st.teps_edges
+        cverts += st.comp_vertices
+        ran += st.sources - st.skipped
+    clk = clocks.stop()
+    barrier()
+    tot_ms = sum(step_ms)
+    tot_edges = edges
+    if dist is not None:
+        t = torch.tensor([tot_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_ms = float(t.item())
+        e = torch.tensor([tot_edges], dtype=torch.float64, device="cuda")
+        dist.all_reduce(e)
+        tot_edges = float(e.item())
+    value = tot_edges / (tot_ms / 1e3)
+
+    # ---- roofline of the sweep kernel (this rank)
+    peak, peak_kind = measured_peak()
+    alg_bytes = 16.0 * edges + 56.0 * cverts + 8.0 * ran
+    kern_s = sum(kern_ms) / 1e3
+    achieved = alg_bytes / kern_s / 1e9
+    tps, tnote = traffic_per_source()
+    traffic = tps * (ran / args.steps) if tps is not None else None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_kind": peak_kind, "traffic": traffic,
+                "alg_bytes_per_launch": alg_bytes / args.steps, "kernel_ms_per_launch": 1e3 * kern_s / args.steps}
+    if tnote:
+        roofline["traffic_note"] = tnote
+
+    # ---- e2e through the C ABI with host buffers
+    e2e_steps = args.e2e_steps or min(args.steps, 3)
+    h_offs = torch.from_numpy(offs).pin_memory().numpy()
+    h_adj = torch.from_numpy(adj).pin_memory().numpy()
+    h_bc = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+    barrier()
+    e2e_ms, e2e_edges = [], 0
+    for _ in range(e2e_steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ge = bcg.Graph(h_offs, h_adj, bcg.PRUNE_DEGREE1)
+        st = ge.run(srcs)
+        if dist is not None:
+            bt = torch.as_tensor(bcg.DeviceArray(ge.bc_device_ptr(), n), device="cuda")
+            dist.all_reduce(bt)
+        bcg.lib().bcg_get_bc(ge.h, h_bc.ctypes.data_as(bcg._f64p))
+        ge.close()
+        torch.cuda.synchronize()
+        e2e_ms.append(1e3 * (time.perf_counter() - t0))
+        e2e_edges += st.teps_edges
+    e2e_tot = sum(e2e_ms)
+    if dist is not None:
+        t = torch.tensor([e2e_tot, float(e2e_edges)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t[1:2])
+        tm = t[0:1].clone()
+        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        e2e_tot, e2e_edges = float(tm.item()), float(t[1].item())
+    e2e = {"value": e2e_edges / (e2e_tot / 1e3), "unit": "TEPS",
+           "h2d_bytes_per_step": int(4 * (n + 1) + 4 * len(adj) + 4 * len(srcs)),
+           "d2h_bytes_per_step": int(8 * n), "steps": e2e_steps,
+           "path": "bcg_graph_create(host CSR) + bcg_run(host sources) + bcg_get_bc(host)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(offs, adj, srcs)
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": "TEPS", "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+               "config": {"workload": WORKLOAD, "graph": SPEC, "n": n, "m": len(adj) // 2,
+                          "sources_per_gpu": ns, "source_seed": SRC_SEED, "pruning": "degree-1",
+                          "sources_skipped_per_step": int(st.skipped), "batch_width": int(st.batch_width),
+                          "parallelism": f"source-sharded x{world}" if world > 1 else "1 GPU",
+                          "l2": "512 MiB flush write between steps (untimed); graph + state exceed L2"},
+               "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clk,
+               "gpu_launches": args.steps}
+        print(json.dumps(out), flush=True)
+    g.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

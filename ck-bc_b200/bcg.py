@@ -1,0 +1,281 @@
+"""ctypes binding of libbcg.so, the C ABI declared in include/bcg.h.
+
+This is the Python face of the engine used by the tests and bench.py.  It
+loads only the in-tree ``libbcg.so`` (built by ``make -C ck-bc_b200`` or
+``__graft_entry__.build()``) and raises when it is missing: there is no
+Python or CPU fallback for any device entry point.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbcg.so")
+
+OK = 0
+ERR_ARG = -1
+ERR_CUDA = -2
+ERR_OOM = -3
+ERR_OVERFLOW = -4
+ERR_TIMEOUT = -5
+ERR_IO = -6
+ERR_DEPTH = -7
+ERR_RANGE = -8
+ERR_NOGPU = -9
+
+PRUNE_DEGREE1 = 0x1
+DIRECTED = 0x2
+
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_f64p = ctypes.POINTER(ctypes.c_double)
+
+
+class HostCSR(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_uint32), ("nnz", ctypes.c_uint64),
+                ("offsets", _u32p), ("adj", _u32p)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("sources", ctypes.c_uint64), ("skipped", ctypes.c_uint64),
+                ("roots", ctypes.c_uint64), ("batches", ctypes.c_uint64),
+                ("teps_edges", ctypes.c_uint64), ("visited", ctypes.c_uint64),
+                ("comp_vertices", ctypes.c_uint64),
+                ("max_depth", ctypes.c_uint32), ("batch_width", ctypes.c_uint32),
+                ("kernel_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class BcgError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"bcg error {code}: {msg}")
+        self.code = code
+
+
+# Every symbol of include/bcg.h with (restype, argtypes).
+SIGNATURES = {
+    "bcg_csr_read_edgelist": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_uint64, ctypes.c_int,
+                                             ctypes.c_int, ctypes.POINTER(HostCSR)]),
+    "bcg_csr_from_pairs": (ctypes.c_int, [_u64p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int,
+                                          ctypes.POINTER(HostCSR)]),
+    "bcg_csr_generate": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(HostCSR)]),
+    "bcg_csr_write_edgelist": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(HostCSR)]),
+    "bcg_csr_free": (None, [ctypes.POINTER(HostCSR)]),
+    "bcg_sample_sources": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, _u32p]),
+    "bcg_device_count": (ctypes.c_int, []),
+    "bcg_graph_create": (ctypes.c_int, [_u32p, _u32p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint32,
+                                        ctypes.POINTER(ctypes.c_void_p)]),
+    "bcg_graph_create_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+                                               ctypes.c_uint64, ctypes.c_uint32,
+                                               ctypes.POINTER(ctypes.c_void_p)]),
+    "bcg_graph_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "bcg_reset_bc": (ctypes.c_int, [ctypes.c_void_p]),
+    "bcg_run": (ctypes.c_int, [ctypes.c_void_p, _u32p, ctypes.c_uint64, ctypes.POINTER(Stats)]),
+    "bcg_run_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                      ctypes.POINTER(Stats)]),
+    "bcg_get_bc": (ctypes.c_int, [ctypes.c_void_p, _f64p]),
+    "bcg_bc_device_ptr": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "bcg_bc_csr": (ctypes.c_int, [_u32p, _u32p, ctypes.c_uint32, ctypes.c_uint64, _u32p, ctypes.c_uint64,
+                                  ctypes.c_uint32, _f64p, ctypes.POINTER(Stats)]),
+    "bcg_single_source": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, _i32p, _u64p, _f64p]),
+    "bcg_graph_pruning": (ctypes.c_int, [ctypes.c_void_p, _u32p, _u32p]),
+    "bcg_graph_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32),
+                                      ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
+                                      ctypes.POINTER(ctypes.c_uint32)]),
+    "bcg_graph_set_reach": (ctypes.c_int, [ctypes.c_void_p, _u32p]),
+    "bcg_run_weighted": (ctypes.c_int, [ctypes.c_void_p, _u32p, _f64p, _u32p, ctypes.c_uint64,
+                                        ctypes.POINTER(Stats)]),
+    "bcg_set_batch_width": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32]),
+    "bcg_last_error": (ctypes.c_char_p, []),
+}
+
+_LIB = None
+
+
+def lib() -> ctypes.CDLL:
+    """Loads the in-tree libbcg.so (raises if it has not been built)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is not built; run `make -C ck-bc_b200` "
+                               "or __graft_entry__.build()")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def _check(rc: int):
+    if rc != OK:
+        msg = lib().bcg_last_error()
+        raise BcgError(rc, msg.decode() if msg else "")
+
+
+def _p32(a: np.ndarray):
+    return a.ctypes.data_as(_u32p)
+
+
+def _take_csr(h: HostCSR):
+    n, nnz = h.n, h.nnz
+    offs = np.ctypeslib.as_array(h.offsets, shape=(n + 1,)).copy()
+    adj = np.ctypeslib.as_array(h.adj, shape=(max(nnz, 1),))[:nnz].copy() if nnz else np.zeros(0, np.uint32)
+    lib().bcg_csr_free(ctypes.byref(h))
+    return offs, adj
+
+
+def generate(spec: str):
+    """Seeded synthetic graph -> (offsets uint32[n+1], adj uint32[nnz])."""
+    h = HostCSR()
+    _check(lib().bcg_csr_generate(spec.encode(), ctypes.byref(h)))
+    return _take_csr(h)
+
+
+def read_edgelist(path: str, n: int, undirected: bool = True, echo_header: bool = False):
+    h = HostCSR()
+    _check(lib().bcg_csr_read_edgelist(os.fsencode(path), n, int(undirected), int(echo_header),
+                                       ctypes.byref(h)))
+    return _take_csr(h)
+
+
+def from_pairs(pairs, n: int, undirected: bool = True):
+    p = np.ascontiguousarray(np.asarray(pairs, dtype=np.uint64).reshape(-1))
+    h = HostCSR()
+    _check(lib().bcg_csr_from_pairs(p.ctypes.data_as(_u64p), p.size // 2, n, int(undirected),
+                                    ctypes.byref(h)))
+    return _take_csr(h)
+
+
+def write_edgelist(path: str, offsets: np.ndarray, adj: np.ndarray):
+    offsets = np.ascontiguousarray(offsets, dtype=np.uint32)
+    adj = np.ascontiguousarray(adj, dtype=np.uint32)
+    h = HostCSR(len(offsets) - 1, len(adj), _p32(offsets), _p32(adj))
+    _check(lib().bcg_csr_write_edgelist(os.fsencode(path), ctypes.byref(h)))
+
+
+def sample_sources(n: int, k: int, seed: int) -> np.ndarray:
+    out = np.zeros(k, dtype=np.uint32)
+    _check(lib().bcg_sample_sources(n, k, seed, _p32(out)))
+    return out
+
+
+def device_count() -> int:
+    return lib().bcg_device_count()
+
+
+class Graph:
+    """One graph resident on the current CUDA device (bcg_graph handle)."""
+
+    def __init__(self, offsets: np.ndarray, adj: np.ndarray, flags: int = 0):
+        self.offsets = np.ascontiguousarray(offsets, dtype=np.uint32)
+        self.adj = np.ascontiguousarray(adj, dtype=np.uint32)
+        self.n = len(self.offsets) - 1
+        self.nnz = len(self.adj)
+        h = ctypes.c_void_p()
+        _check(lib().bcg_graph_create(_p32(self.offsets), _p32(self.adj) if self.nnz else None,
+                                      self.n, self.nnz, flags, ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            lib().bcg_graph_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def reset(self):
+        _check(lib().bcg_reset_bc(self.h))
+
+    def run(self, sources) -> Stats:
+        s = np.ascontiguousarray(sources, dtype=np.uint32)
+        st = Stats()
+        _check(lib().bcg_run(self.h, _p32(s), len(s), ctypes.byref(st)))
+        return st
+
+    def run_device(self, d_sources_ptr: int, nsrc: int, stream: int = 0, stats: bool = False):
+        st = Stats() if stats else None
+        _check(lib().bcg_run_device(self.h, ctypes.c_void_p(d_sources_ptr), nsrc, ctypes.c_void_p(stream),
+                                    ctypes.byref(st) if st is not None else None))
+        return st
+
+    def bc(self) -> np.ndarray:
+        out = np.zeros(self.n, dtype=np.float64)
+        _check(lib().bcg_get_bc(self.h, out.ctypes.data_as(_f64p)))
+        return out
+
+    def bc_device_ptr(self) -> int:
+        p = ctypes.c_void_p()
+        _check(lib().bcg_bc_device_ptr(self.h, ctypes.byref(p)))
+        return p.value
+
+    def single_source(self, src: int):
+        lvl = np.zeros(self.n, dtype=np.int32)
+        sig = np.zeros(self.n, dtype=np.uint64)
+        dl = np.zeros(self.n, dtype=np.float64)
+        _check(lib().bcg_single_source(self.h, src, lvl.ctypes.data_as(_i32p), sig.ctypes.data_as(_u64p),
+                                       dl.ctypes.data_as(_f64p)))
+        return lvl, sig, dl
+
+    def pruning(self):
+        anc = np.zeros(self.n, dtype=np.uint32)
+        rch = np.zeros(self.n, dtype=np.uint32)
+        _check(lib().bcg_graph_pruning(self.h, _p32(anc), _p32(rch)))
+        return anc, rch
+
+    def info(self):
+        n = ctypes.c_uint32()
+        nnz = ctypes.c_uint64()
+        nnzp = ctypes.c_uint64()
+        npr = ctypes.c_uint32()
+        _check(lib().bcg_graph_info(self.h, ctypes.byref(n), ctypes.byref(nnz), ctypes.byref(nnzp),
+                                    ctypes.byref(npr)))
+        return {"n": n.value, "nnz": nnz.value, "nnz_pruned": nnzp.value, "pruned": npr.value}
+
+    def set_batch_width(self, w: int):
+        _check(lib().bcg_set_batch_width(self.h, w))
+
+
+def bc_csr(offsets, adj, sources, flags: int = 0):
+    """One-shot drop-in call on host buffers -> (bc float64[n], Stats)."""
+    offsets = np.ascontiguousarray(offsets, dtype=np.uint32)
+    adj = np.ascontiguousarray(adj, dtype=np.uint32)
+    s = np.ascontiguousarray(sources, dtype=np.uint32)
+    n = len(offsets) - 1
+    out = np.zeros(n, dtype=np.float64)
+    st = Stats()
+    _check(lib().bcg_bc_csr(_p32(offsets), _p32(adj) if len(adj) else None, n, len(adj), _p32(s), len(s),
+                            flags, out.ctypes.data_as(_f64p), ctypes.byref(st)))
+    return out, st
+
+
+@dataclass
+class DeviceArray:
+    """Exposes a raw device pointer through __cuda_array_interface__ so that
+    torch.as_tensor(..., device='cuda') wraps it without a copy."""
+    ptr: int
+    n: int
+    typestr: str = "<f8"
+
+    @property
+    def __cuda_array_interface__(self):
+        return {"shape": (self.n,), "typestr": self.typestr, "data": (self.ptr, False), "version": 3,
+                "strides": None}

@@ -1,0 +1,127 @@
+// libbc2d_compat.so: the reference's bc2d.h mono-path ABI (include/bc2d_compat.h)
+// implemented on libbcg.  Errors print and exit like the reference's
+// MY_CUDA_CHECK (cudamacro.h:1-7), since the ABI has no status returns.
+#include <cuda_runtime.h>
+
+#include <cinttypes>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "bc2d_compat.h"
+#include "bcg.h"
+
+extern "C" {
+extern uint64_t N;  // vertex count, defined by the reference's bc2d.c
+}
+
+namespace {
+
+bcg_graph *g_graph = nullptr;
+std::vector<uint32_t> g_deg;       // degree of every vertex (CSC column lengths)
+std::vector<int32_t> g_level;      // BFS depth of the current source (-1 = not reached)
+std::vector<uint32_t> g_count;     // vertices per level of the current source
+uint32_t g_v0 = 0;
+uint32_t g_reach_v0 = 0;
+
+[[noreturn]] void fail(const char *what, int rc) {
+    fprintf(stderr, "bc2d_compat: %s failed (%d): %s\n", what, rc, bcg_last_error());
+    exit(EXIT_FAILURE);
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t initcuda(uint64_t ned, LOCINT *col, LOCINT *row) {
+    const uint32_t n = (uint32_t)N;
+    int rc = bcg_graph_create(col, row, n, ned, 0u, &g_graph);
+    if (rc) fail("initcuda", rc);
+    g_deg.resize(n);
+    for (uint32_t v = 0; v < n; ++v) g_deg[v] = col[v + 1] - col[v];
+    g_level.assign(n, -1);
+    printf("ROWBL = %i - ROWPP = %i\n", (int)n, (int)n);
+    return (size_t)(n + 1) * 4 + ned * 4 + (size_t)n * (8 + 8 + 16);
+}
+
+void init_bc_1degree_device(LOCINT *reach) {
+    int rc = bcg_graph_set_reach(g_graph, reach);
+    if (rc) fail("init_bc_1degree_device", rc);
+}
+
+void get_deg(LOCINT *deg) { memcpy(deg, g_deg.data(), g_deg.size() * sizeof(uint32_t)); }
+
+void setcuda(uint64_t, LOCINT *, LOCINT *, LOCINT reach_v0) {
+    g_reach_v0 = reach_v0;
+    g_count.clear();
+}
+
+void set_mlp_cuda(LOCINT row, int, int) {
+    g_v0 = row;
+    int rc = bcg_single_source(g_graph, row, g_level.data(), nullptr, nullptr);
+    if (rc) fail("set_mlp_cuda", rc);
+    g_count.clear();
+    for (int32_t l : g_level) {
+        if (l < 0) continue;
+        if ((size_t)l >= g_count.size()) g_count.resize(l + 1, 0);
+        ++g_count[l];
+    }
+}
+
+LOCINT scan_col_csc_cuda_mono(int, int level) {
+    return (level >= 0 && (size_t)level < g_count.size()) ? g_count[level] : 0u;
+}
+
+LOCINT scan_frt_csc_cuda_mono(int, int ncol, int) { return (LOCINT)ncol; }
+
+void pre_update_bc_cuda(LOCINT *reach, uint64_t, LOCINT *all) {
+    uint64_t s = 0;
+    for (size_t v = 0; v < g_level.size(); ++v)
+        if (g_level[v] > 0) s += reach[v];
+    *all = (LOCINT)s;
+}
+
+void update_bc_cuda(uint64_t v0, int, const uint64_t) {
+    const uint32_t root = (uint32_t)v0;
+    const double mult = (double)g_reach_v0 + 1.0;
+    const uint32_t pend = g_reach_v0;
+    int rc = bcg_run_weighted(g_graph, &root, &mult, &pend, 1, nullptr);
+    if (rc) fail("update_bc_cuda", rc);
+}
+
+void get_msk(LOCINT *msk) {
+    const size_t n = g_level.size();
+    memset(msk, 0, ((n + 31) / 32) * sizeof(uint32_t));
+    for (size_t v = 0; v < n; ++v)
+        if (g_level[v] >= 0) msk[v / 32] |= 1u << (v % 32);
+}
+
+void get_bc(float *bc) {
+    std::vector<double> b(g_deg.size());
+    int rc = bcg_get_bc(g_graph, b.data());
+    if (rc) fail("get_bc", rc);
+    for (size_t v = 0; v < b.size(); ++v) bc[v] = (float)b[v];
+}
+
+void fincuda(void) {
+    if (g_graph) bcg_graph_destroy(g_graph);
+    g_graph = nullptr;
+}
+
+void *CudaMallocHostSet(size_t size, int val) {
+    void *p = nullptr;
+    cudaError_t e = cudaMallocHost(&p, size);
+    if (e != cudaSuccess) {
+        fprintf(stderr, "Cuda error in CudaMallocHostSet : %s.\n", cudaGetErrorString(e));
+        exit(EXIT_FAILURE);
+    }
+    memset(p, val, size);
+    return p;
+}
+
+void CudaFreeHost(void *ptr) {
+    if (ptr) cudaFreeHost(ptr);
+}
+
+}  // extern "C"

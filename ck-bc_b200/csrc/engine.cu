@@ -1,0 +1,677 @@
+// Graph handle, degree-1 pruning pre-pass, work tiles and the bcg_* C ABI.
+//
+// Reference counterparts:
+//   initcuda / fincuda            cuda_kernels.cu:1123-1198, 1201-1232
+//   degree_reduction              bc2d.c:314-419   (host qsort + merge, one layer)
+//   init_bc_1degree(_device)      bc2d.c:455-465, cuda_kernels.cu:1083-1087
+//   per-source loop + skip        bc2d.c:1016-1050
+//   get_bc                        cuda_kernels.cu:1039-1041
+//
+// Degree-1 pruning (north_star (a)).  A vertex p of degree 1 whose neighbour a
+// does not also have degree 1 is folded into a: p leaves the traversal graph
+// and reach[a] counts it.  For an isolated edge {p, a} (both degree 1) the
+// larger id is folded into the smaller.  The pruned graph keeps the vertex
+// ids and the CSR row starts; each surviving list is compacted to the front of
+// its row and vinfo[v].x holds its new length.  Exact BC is preserved by
+// weighting (derivation in DESIGN.md):
+//   - the backward pass starts every delta at reach[v] (init_delta,
+//     cuda_kernels.cu:1089-1098), so pendants count as targets;
+//   - a source s folded into anchor a runs as a BFS from a; the root's
+//     dependencies are added mult(a) = [a requested] + #(requested pendants of
+//     a) times;
+//   - the root gets pend(a) * (W - 2), W = number of original vertices of its
+//     component (update_bc's source term, cuda_kernels.cu:269-271).
+// Unlike the reference, a vertex whose every neighbour was folded (isolated in
+// the pruned graph) is still run as a root, and vertices outside the root's
+// component get nothing (the reference adds reach * (reach_v0 + 1) to them,
+// cuda_kernels.cu:274, 1095).
+#include <algorithm>
+#include <cinttypes>
+#include <cstdlib>
+#include <cstring>
+#include <unordered_map>
+#include <vector>
+
+#include "bcg_common.hpp"
+#include "engine.cuh"
+
+namespace bcg {
+
+int launch_sweep(int S, const BatchArgs &a, cudaStream_t st, int *grid_out);
+
+#define CK(call)                                                                           \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return set_error(e_ == cudaErrorMemoryAllocation ? BCG_ERR_OOM : BCG_ERR_CUDA, \
+                             "%s failed: %s", #call, cudaGetErrorString(e_));             \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// Pruning kernels.
+// ---------------------------------------------------------------------------
+
+__global__ void k_prune_mark(uint32_t n, const uint32_t *__restrict__ offs, const uint32_t *__restrict__ adj,
+                             uint32_t *__restrict__ anchor, uint32_t *__restrict__ reach) {
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    uint32_t anc = v;
+    if (offs[v + 1] - offs[v] == 1) {
+        const uint32_t a = adj[offs[v]];
+        const bool pair = (offs[a + 1] - offs[a] == 1);
+        if (!(pair && v < a)) {
+            anc = a;
+            atomicAdd(reach + a, 1u);
+        }
+    }
+    anchor[v] = anc;
+}
+
+// One warp per vertex: drop folded neighbours from the list (order kept).
+__global__ void k_prune_compact(uint32_t n, const uint32_t *__restrict__ offs, uint32_t *__restrict__ adj,
+                                const uint32_t *__restrict__ anchor, const uint32_t *__restrict__ reach,
+                                uint2 *__restrict__ vinfo) {
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    const uint32_t v = warp;
+    const uint32_t b = offs[v], e = offs[v + 1];
+    const uint32_t r = reach[v];
+    if (anchor[v] != v) {
+        if (lane == 0) vinfo[v] = make_uint2(0u, 0u);
+        return;
+    }
+    if (r == 0) {
+        if (lane == 0) vinfo[v] = make_uint2(e - b, 0u);
+        return;
+    }
+    uint32_t out = b;
+    for (uint32_t base = b; base < e; base += 32) {
+        const uint32_t i = base + lane;
+        uint32_t w = 0;
+        bool keep = false;
+        if (i < e) {
+            w = adj[i];
+            keep = (anchor[w] == w);
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        __syncwarp();
+        if (keep) adj[out + __popc(bal & ((1u << lane) - 1u))] = w;
+        out += __popc(bal);
+        __syncwarp();
+    }
+    if (lane == 0) vinfo[v] = make_uint2(out - b, r);
+}
+
+__global__ void k_vinfo_plain(uint32_t n, const uint32_t *__restrict__ offs, uint2 *__restrict__ vinfo) {
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < n) vinfo[v] = make_uint2(offs[v + 1] - offs[v], 0u);
+}
+
+__global__ void k_levels_out(uint32_t n, const uint16_t *__restrict__ lvl, int32_t *__restrict__ out) {
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < n) out[v] = lvl[v] == kUnvisited ? -1 : (int32_t)lvl[v];
+}
+
+// ---------------------------------------------------------------------------
+// Work tiles (host, from the original row starts).
+// ---------------------------------------------------------------------------
+
+static void build_tiles(const uint32_t *offs, uint32_t n, std::vector<Tile> &tiles, uint32_t &nhub) {
+    tiles.clear();
+    nhub = 0;
+    uint32_t v = 0;
+    while (v < n) {
+        const uint32_t dv = offs[v + 1] - offs[v];
+        if (dv > (uint32_t)kTileEdges) {
+            const uint32_t nch = (dv + kTileEdges - 1) / kTileEdges;
+            for (uint32_t c = 0; c < nch; ++c) {
+                Tile t{};
+                t.v0 = v; t.v1 = v + 1;
+                t.e0 = offs[v] + c * kTileEdges;
+                t.e1 = std::min(offs[v + 1], t.e0 + (uint32_t)kTileEdges);
+                t.hub = (int32_t)nhub;
+                t.nchunks = nch;
+                tiles.push_back(t);
+            }
+            ++nhub;
+            ++v;
+            continue;
+        }
+        const uint32_t start = v;
+        uint32_t sum = 0;
+        while (v < n && v - start < (uint32_t)kTileVerts) {
+            const uint32_t d = offs[v + 1] - offs[v];
+            if (d > (uint32_t)kTileEdges || sum + d > (uint32_t)kTileEdges) break;
+            sum += d;
+            ++v;
+        }
+        Tile t{};
+        t.v0 = start; t.v1 = v;
+        t.e0 = offs[start]; t.e1 = offs[v];
+        t.hub = -1;
+        t.nchunks = 1;
+        tiles.push_back(t);
+    }
+}
+
+}  // namespace bcg
+
+using namespace bcg;
+
+struct bcg_graph {
+    int device = 0;
+    uint32_t n = 0;
+    uint64_t nnz = 0, nnz_pruned = 0;
+    uint32_t flags = 0;
+    uint32_t npruned = 0;
+    uint32_t *d_offs = nullptr, *d_adj = nullptr;
+    uint2 *d_vinfo = nullptr;
+    uint32_t *d_anchor = nullptr, *d_reach = nullptr;
+    double *d_bc = nullptr;
+    Tile *d_tiles = nullptr;
+    uint32_t ntiles = 0, nhub = 0;
+    unsigned long long *d_hub_acc = nullptr;
+    unsigned int *d_hub_cnt = nullptr;
+    uint16_t *d_lvl = nullptr;
+    unsigned long long *d_val = nullptr;
+    uint32_t state_width = 0;
+    Ctrl *d_ctrl = nullptr;
+    uint32_t *d_roots = nullptr, *d_pend = nullptr;
+    double *d_mult = nullptr;
+    RootStat *d_rstat = nullptr;
+    size_t run_cap = 0;
+    std::vector<uint32_t> h_deg;     // original degree (source skip test)
+    std::vector<uint32_t> h_anchor;  // empty when not pruned
+    uint32_t forced_width = 0;
+    float ratio = 0.5f;
+    unsigned long long wait_ns = kDefaultWaitNs;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace bcg {
+
+static void graph_free(bcg_graph *g) {
+    if (!g) return;
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (cur != g->device) cudaSetDevice(g->device);
+    cudaFree(g->d_offs); cudaFree(g->d_adj); cudaFree(g->d_vinfo);
+    cudaFree(g->d_anchor); cudaFree(g->d_reach); cudaFree(g->d_bc);
+    cudaFree(g->d_tiles); cudaFree(g->d_hub_acc); cudaFree(g->d_hub_cnt);
+    cudaFree(g->d_lvl); cudaFree(g->d_val); cudaFree(g->d_ctrl);
+    cudaFree(g->d_roots); cudaFree(g->d_pend); cudaFree(g->d_mult); cudaFree(g->d_rstat);
+    if (g->ev0) cudaEventDestroy(g->ev0);
+    if (g->ev1) cudaEventDestroy(g->ev1);
+    if (cur >= 0 && cur != g->device) cudaSetDevice(cur);
+    delete g;
+}
+
+static int ensure_state(bcg_graph *g, uint32_t S) {
+    if (g->state_width >= S) return BCG_OK;
+    cudaFree(g->d_lvl); g->d_lvl = nullptr;
+    cudaFree(g->d_val); g->d_val = nullptr;
+    cudaFree(g->d_hub_acc); g->d_hub_acc = nullptr;
+    g->state_width = 0;
+    CK(cudaMalloc(&g->d_lvl, (size_t)g->n * S * sizeof(uint16_t)));
+    CK(cudaMalloc(&g->d_val, (size_t)g->n * S * sizeof(unsigned long long)));
+    CK(cudaMalloc(&g->d_hub_acc, (size_t)std::max(1u, g->nhub) * S * sizeof(unsigned long long)));
+    CK(cudaMemset(g->d_hub_acc, 0, (size_t)std::max(1u, g->nhub) * S * sizeof(unsigned long long)));
+    g->state_width = S;
+    return BCG_OK;
+}
+
+static int ensure_run(bcg_graph *g, size_t slots) {
+    if (g->run_cap >= slots) return BCG_OK;
+    cudaFree(g->d_roots); cudaFree(g->d_pend); cudaFree(g->d_mult); cudaFree(g->d_rstat);
+    g->d_roots = g->d_pend = nullptr; g->d_mult = nullptr; g->d_rstat = nullptr;
+    g->run_cap = 0;
+    size_t cap = std::max<size_t>(slots, 64);
+    CK(cudaMalloc(&g->d_roots, cap * sizeof(uint32_t)));
+    CK(cudaMalloc(&g->d_pend, cap * sizeof(uint32_t)));
+    CK(cudaMalloc(&g->d_mult, cap * sizeof(double)));
+    CK(cudaMalloc(&g->d_rstat, cap * sizeof(RootStat)));
+    g->run_cap = cap;
+    return BCG_OK;
+}
+
+// Sources per batch: the widest S in {8,4,2,1} whose per-vertex state
+// (S * (2 + 8) bytes) fits the L2-resident budget, and not wider than needed.
+static uint32_t choose_width(const bcg_graph *g, uint64_t nroots) {
+    if (g->forced_width) return g->forced_width;
+    double budget = 56.0 * 1024 * 1024;
+    if (const char *e = getenv("BCG_STATE_BUDGET_MB")) budget = atof(e) * 1024 * 1024;
+    uint32_t S = 8;
+    while (S > 1 && (double)g->n * S * 10.0 > budget) S >>= 1;
+    while (S > 1 && (uint64_t)(S >> 1) >= nroots) S >>= 1;
+    return S;
+}
+
+static int create_common(bcg_graph *g, const uint32_t *h_offs) {
+    const uint32_t n = g->n;
+    CK(cudaMalloc(&g->d_vinfo, (size_t)n * sizeof(uint2)));
+    CK(cudaMalloc(&g->d_bc, (size_t)n * sizeof(double)));
+    CK(cudaMemset(g->d_bc, 0, (size_t)n * sizeof(double)));
+    CK(cudaMalloc(&g->d_ctrl, sizeof(Ctrl)));
+    CK(cudaEventCreate(&g->ev0));
+    CK(cudaEventCreate(&g->ev1));
+    g->h_deg.resize(n);
+    for (uint32_t v = 0; v < n; ++v) g->h_deg[v] = h_offs[v + 1] - h_offs[v];
+    const bool prune = (g->flags & BCG_PRUNE_DEGREE1) && !(g->flags & BCG_DIRECTED);
+    const unsigned nb = (n + 255) / 256;
+    if (prune) {
+        CK(cudaMalloc(&g->d_anchor, (size_t)n * sizeof(uint32_t)));
+        CK(cudaMalloc(&g->d_reach, (size_t)n * sizeof(uint32_t)));
+        CK(cudaMemset(g->d_reach, 0, (size_t)n * sizeof(uint32_t)));
+        k_prune_mark<<<nb, 256>>>(n, g->d_offs, g->d_adj, g->d_anchor, g->d_reach);
+        CK(cudaGetLastError());
+        const uint64_t threads = (uint64_t)n * 32;
+        k_prune_compact<<<(unsigned)((threads + 255) / 256), 256>>>(n, g->d_offs, g->d_adj, g->d_anchor,
+                                                                    g->d_reach, g->d_vinfo);
+        CK(cudaGetLastError());
+        g->h_anchor.resize(n);
+        CK(cudaMemcpy(g->h_anchor.data(), g->d_anchor, (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        uint32_t np = 0;
+        for (uint32_t v = 0; v < n; ++v) np += (g->h_anchor[v] != v);
+        g->npruned = np;
+        g->nnz_pruned = g->nnz - 2ull * np;
+    } else {
+        k_vinfo_plain<<<nb, 256>>>(n, g->d_offs, g->d_vinfo);
+        CK(cudaGetLastError());
+        g->nnz_pruned = g->nnz;
+    }
+    std::vector<Tile> tiles;
+    build_tiles(h_offs, n, tiles, g->nhub);
+    g->ntiles = (uint32_t)tiles.size();
+    CK(cudaMalloc(&g->d_tiles, std::max<size_t>(1, tiles.size()) * sizeof(Tile)));
+    if (!tiles.empty())
+        CK(cudaMemcpy(g->d_tiles, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&g->d_hub_cnt, (size_t)std::max(1u, g->nhub) * sizeof(unsigned int)));
+    CK(cudaMemset(g->d_hub_cnt, 0, (size_t)std::max(1u, g->nhub) * sizeof(unsigned int)));
+    CK(cudaDeviceSynchronize());
+    return BCG_OK;
+}
+
+static int check_device() {
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+        return set_error(BCG_ERR_NOGPU, "no CUDA device: %s", e == cudaSuccess ? "0 devices" : cudaGetErrorString(e));
+    return BCG_OK;
+}
+
+static int validate_csr(const uint32_t *offs, const uint32_t *adj, uint32_t n, uint64_t nnz) {
+    if (offs[0] != 0 || offs[n] != nnz) return set_error(BCG_ERR_ARG, "offsets[0] must be 0 and offsets[n] == nnz");
+    for (uint32_t v = 0; v < n; ++v)
+        if (offs[v + 1] < offs[v]) return set_error(BCG_ERR_ARG, "offsets not non-decreasing at %u", v);
+    for (uint64_t e = 0; e < nnz; ++e)
+        if (adj[e] >= n) return set_error(BCG_ERR_ARG, "adj[%" PRIu64 "] = %u >= n", e, adj[e]);
+    return BCG_OK;
+}
+
+struct RunPlan {
+    std::vector<uint32_t> roots, pend;
+    std::vector<double> mult;
+    std::vector<uint64_t> count;  // sources mapped to each root
+    uint64_t skipped = 0;
+};
+
+static int plan_run(const bcg_graph *g, const uint32_t *src, uint64_t nsrc, RunPlan &p) {
+    std::unordered_map<uint32_t, uint32_t> idx;
+    idx.reserve(nsrc * 2 + 1);
+    for (uint64_t i = 0; i < nsrc; ++i) {
+        const uint32_t s = src[i];
+        if (s >= g->n) return set_error(BCG_ERR_ARG, "source %u >= n=%u", s, g->n);
+        if (g->h_deg[s] == 0) { ++p.skipped; continue; }
+        const uint32_t r = g->h_anchor.empty() ? s : g->h_anchor[s];
+        auto it = idx.find(r);
+        uint32_t k;
+        if (it == idx.end()) {
+            k = (uint32_t)p.roots.size();
+            idx.emplace(r, k);
+            p.roots.push_back(r);
+            p.pend.push_back(0);
+            p.mult.push_back(0.0);
+            p.count.push_back(0);
+        } else {
+            k = it->second;
+        }
+        p.mult[k] += 1.0;
+        p.count[k] += 1;
+        if (r != s) p.pend[k] += 1;
+    }
+    return BCG_OK;
+}
+
+static int run_plan(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *stats, bool debug,
+                    unsigned long long *dbg_sigma, double *dbg_delta) {
+    const uint64_t nroots = p.roots.size();
+    if (stats) {
+        stats->skipped = p.skipped;
+        stats->roots = nroots;
+    }
+    if (nroots == 0) return BCG_OK;
+    const uint32_t S = debug ? 1u : choose_width(g, nroots);
+    int rc = ensure_state(g, S);
+    if (rc) return rc;
+    const uint64_t nbatch = (nroots + S - 1) / S;
+    const size_t slots = nbatch * S;
+    rc = ensure_run(g, slots);
+    if (rc) return rc;
+    std::vector<uint32_t> roots(slots, kNoRoot), pend(slots, 0);
+    std::vector<double> mult(slots, 0.0);
+    for (uint64_t i = 0; i < nroots; ++i) { roots[i] = p.roots[i]; pend[i] = p.pend[i]; mult[i] = p.mult[i]; }
+    CK(cudaMemcpyAsync(g->d_roots, roots.data(), slots * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(g->d_pend, pend.data(), slots * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(g->d_mult, mult.data(), slots * sizeof(double), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(g->d_ctrl, 0, sizeof(Ctrl), st));
+    CK(cudaMemsetAsync(g->d_hub_acc, 0, (size_t)std::max(1u, g->nhub) * g->state_width * sizeof(unsigned long long), st));
+    CK(cudaMemsetAsync(g->d_hub_cnt, 0, (size_t)std::max(1u, g->nhub) * sizeof(unsigned int), st));
+    CK(cudaMemcpyAsync(&g->d_ctrl->wait_ns, &g->wait_ns, sizeof(unsigned long long), cudaMemcpyHostToDevice, st));
+    BatchArgs a{};
+    a.n = g->n;
+    a.offs = g->d_offs;
+    a.adj = g->d_adj;
+    a.vinfo = g->d_vinfo;
+    a.tiles = g->d_tiles;
+    a.ntiles = g->ntiles;
+    a.lvl = g->d_lvl;
+    a.val = g->d_val;
+    a.bc = g->d_bc;
+    a.roots = g->d_roots;
+    a.mult = g->d_mult;
+    a.pend = g->d_pend;
+    a.nbatch = (uint32_t)nbatch;
+    a.hub_acc = g->d_hub_acc;
+    a.hub_cnt = g->d_hub_cnt;
+    a.ctrl = g->d_ctrl;
+    a.rstat = g->d_rstat;
+    a.nnz = g->nnz_pruned;
+    a.push_pull_ratio = g->ratio;
+    a.directed = (g->flags & BCG_DIRECTED) ? 1 : 0;
+    a.dbg_sigma = dbg_sigma;
+    a.dbg_delta = dbg_delta;
+    CK(cudaEventRecord(g->ev0, st));
+    int grid = 0;
+    rc = launch_sweep((int)S, a, st, &grid);
+    if (rc) return rc;
+    CK(cudaEventRecord(g->ev1, st));
+    if (!stats && !debug) return BCG_OK;
+    CK(cudaStreamSynchronize(st));
+    Ctrl c{};
+    CK(cudaMemcpy(&c, g->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+    if (c.error) return set_error(c.error, "device reported error %d (%s)", c.error,
+                                  c.error == BCG_ERR_TIMEOUT ? "a bounded wait gave up" : "level limit exceeded");
+    if (c.overflow) return set_error(BCG_ERR_OVERFLOW, "a shortest-path count exceeded 2^64");
+    if (stats) {
+        std::vector<RootStat> rs(slots);
+        CK(cudaMemcpy(rs.data(), g->d_rstat, slots * sizeof(RootStat), cudaMemcpyDeviceToHost));
+        uint64_t teps = 0, vis = 0, cv = 0;
+        uint32_t md = 0;
+        for (uint64_t i = 0; i < nroots; ++i) {
+            teps += p.count[i] * (rs[i].mc2 / 2);
+            cv += p.count[i] * rs[i].wsum;
+            vis += rs[i].visited;
+            md = std::max(md, rs[i].depth);
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, g->ev0, g->ev1);
+        stats->batches = nbatch;
+        stats->teps_edges = teps;
+        stats->visited = vis;
+        stats->comp_vertices = cv;
+        stats->max_depth = md;
+        stats->batch_width = S;
+        stats->kernel_ms = ms;
+    }
+    return BCG_OK;
+}
+
+}  // namespace bcg
+
+extern "C" {
+
+int bcg_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint32_t n, uint64_t nnz,
+                             uint32_t flags, bool device_in, bcg_graph **out) {
+    clear_error();
+    if (!out) return set_error(BCG_ERR_ARG, "null output handle");
+    *out = nullptr;
+    if (!offsets || (nnz && !adj) || n == 0) return set_error(BCG_ERR_ARG, "null CSR or n == 0");
+    if (nnz > 0xFFFFFFFFull || n > 0xFFFFFFFEu) return set_error(BCG_ERR_RANGE, "graph exceeds 32-bit ids/offsets");
+    int rc = check_device();
+    if (rc) return rc;
+    std::vector<uint32_t> h_offs;
+    const uint32_t *ho = offsets;
+    if (device_in) {
+        h_offs.resize((size_t)n + 1);
+        cudaError_t e = cudaMemcpy(h_offs.data(), offsets, ((size_t)n + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return set_error(BCG_ERR_CUDA, "reading offsets: %s", cudaGetErrorString(e));
+        ho = h_offs.data();
+        if (ho[0] != 0 || ho[n] != nnz) return set_error(BCG_ERR_ARG, "offsets[0] must be 0 and offsets[n] == nnz");
+        for (uint32_t v = 0; v < n; ++v)
+            if (ho[v + 1] < ho[v]) return set_error(BCG_ERR_ARG, "offsets not non-decreasing at %u", v);
+    } else {
+        rc = validate_csr(offsets, adj, n, nnz);
+        if (rc) return rc;
+    }
+    bcg_graph *g = new bcg_graph();
+    cudaGetDevice(&g->device);
+    g->n = n;
+    g->nnz = nnz;
+    g->flags = flags;
+    if (const char *e = getenv("BCG_PUSH_PULL_RATIO")) g->ratio = (float)atof(e);
+    auto fail = [&](int code) { graph_free(g); return code; };
+    cudaError_t e;
+    if ((e = cudaMalloc(&g->d_offs, ((size_t)n + 1) * sizeof(uint32_t))) != cudaSuccess ||
+        (e = cudaMalloc(&g->d_adj, std::max<uint64_t>(nnz, 1) * sizeof(uint32_t))) != cudaSuccess)
+        return fail(set_error(BCG_ERR_OOM, "cudaMalloc CSR: %s", cudaGetErrorString(e)));
+    const cudaMemcpyKind kind = device_in ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    if ((e = cudaMemcpy(g->d_offs, offsets, ((size_t)n + 1) * sizeof(uint32_t), kind)) != cudaSuccess ||
+        (nnz && (e = cudaMemcpy(g->d_adj, adj, nnz * sizeof(uint32_t), kind)) != cudaSuccess))
+        return fail(set_error(BCG_ERR_CUDA, "uploading CSR: %s", cudaGetErrorString(e)));
+    rc = create_common(g, ho);
+    if (rc) return fail(rc);
+    *out = g;
+    return BCG_OK;
+}
+
+int bcg_graph_create(const uint32_t *offsets, const uint32_t *adj, uint32_t n, uint64_t nnz, uint32_t flags,
+                     bcg_graph **out) {
+    return graph_create_impl(offsets, adj, n, nnz, flags, false, out);
+}
+
+int bcg_graph_create_device(const uint32_t *d_offsets, const uint32_t *d_adj, uint32_t n, uint64_t nnz,
+                            uint32_t flags, bcg_graph **out) {
+    return graph_create_impl(d_offsets, d_adj, n, nnz, flags, true, out);
+}
+
+int bcg_graph_destroy(bcg_graph *g) {
+    clear_error();
+    if (!g) return set_error(BCG_ERR_ARG, "null handle");
+    graph_free(g);
+    return BCG_OK;
+}
+
+int bcg_reset_bc(bcg_graph *g) {
+    clear_error();
+    if (!g) return set_error(BCG_ERR_ARG, "null handle");
+    CK(cudaMemset(g->d_bc, 0, (size_t)g->n * sizeof(double)));
+    return BCG_OK;
+}
+
+int bcg_run(bcg_graph *g, const uint32_t *sources, uint64_t nsrc, bcg_stats *stats) {
+    clear_error();
+    if (!g || (nsrc && !sources)) return set_error(BCG_ERR_ARG, "null argument");
+    bcg_stats local{};
+    bcg_stats *st = stats ? stats : &local;
+    *st = bcg_stats{};
+    st->sources = nsrc;
+    RunPlan p;
+    int rc = plan_run(g, sources, nsrc, p);
+    if (rc) return rc;
+    return run_plan(g, p, 0, st, false, nullptr, nullptr);
+}
+
+int bcg_run_device(bcg_graph *g, const uint32_t *d_sources, uint64_t nsrc, void *stream, bcg_stats *stats) {
+    clear_error();
+    if (!g || (nsrc && !d_sources)) return set_error(BCG_ERR_ARG, "null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    std::vector<uint32_t> h(nsrc);
+    if (nsrc) {
+        CK(cudaMemcpyAsync(h.data(), d_sources, nsrc * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    if (stats) { *stats = bcg_stats{}; stats->sources = nsrc; }
+    RunPlan p;
+    int rc = plan_run(g, h.data(), nsrc, p);
+    if (rc) return rc;
+    return run_plan(g, p, st, stats, false, nullptr, nullptr);
+}
+
+int bcg_get_bc(bcg_graph *g, double *bc_host) {
+    clear_error();
+    if (!g || !bc_host) return set_error(BCG_ERR_ARG, "null argument");
+    CK(cudaMemcpy(bc_host, g->d_bc, (size_t)g->n * sizeof(double), cudaMemcpyDeviceToHost));
+    return BCG_OK;
+}
+
+int bcg_bc_device_ptr(bcg_graph *g, double **d_bc) {
+    clear_error();
+    if (!g || !d_bc) return set_error(BCG_ERR_ARG, "null argument");
+    *d_bc = g->d_bc;
+    return BCG_OK;
+}
+
+int bcg_bc_csr(const uint32_t *offsets, const uint32_t *adj, uint32_t n, uint64_t nnz, const uint32_t *sources,
+               uint64_t nsrc, uint32_t flags, double *bc_out, bcg_stats *stats) {
+    clear_error();
+    if (!bc_out) return set_error(BCG_ERR_ARG, "null bc_out");
+    bcg_graph *g = nullptr;
+    int rc = bcg_graph_create(offsets, adj, n, nnz, flags, &g);
+    if (rc) return rc;
+    rc = bcg_run(g, sources, nsrc, stats);
+    if (!rc) rc = bcg_get_bc(g, bc_out);
+    graph_free(g);
+    return rc;
+}
+
+int bcg_single_source(bcg_graph *g, uint32_t src, int32_t *level, uint64_t *sigma, double *delta) {
+    clear_error();
+    if (!g) return set_error(BCG_ERR_ARG, "null handle");
+    if (src >= g->n) return set_error(BCG_ERR_ARG, "source %u >= n=%u", src, g->n);
+    const size_t n = g->n;
+    // the bc accumulator is saved and restored around the run
+    double *d_save = nullptr;
+    unsigned long long *d_sig = nullptr;
+    double *d_del = nullptr;
+    int32_t *d_lvl = nullptr;
+    int rc = BCG_OK;
+    auto cleanup = [&]() { cudaFree(d_save); cudaFree(d_sig); cudaFree(d_del); cudaFree(d_lvl); };
+    if (cudaMalloc(&d_save, n * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&d_sig, n * sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc(&d_del, n * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&d_lvl, n * sizeof(int32_t)) != cudaSuccess) {
+        cleanup();
+        return set_error(BCG_ERR_OOM, "single-source scratch allocation failed");
+    }
+    cudaMemcpy(d_save, g->d_bc, n * sizeof(double), cudaMemcpyDeviceToDevice);
+    cudaMemset(d_sig, 0, n * sizeof(unsigned long long));
+    cudaMemset(d_del, 0, n * sizeof(double));
+    RunPlan p;
+    p.roots.push_back(src);
+    p.pend.push_back(0);
+    p.mult.push_back(1.0);
+    p.count.push_back(1);
+    rc = run_plan(g, p, 0, nullptr, true, d_sig, d_del);
+    if (!rc) {
+        k_levels_out<<<(unsigned)((n + 255) / 256), 256>>>(g->n, g->d_lvl, d_lvl);
+        cudaError_t e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) rc = set_error(BCG_ERR_CUDA, "levels: %s", cudaGetErrorString(e));
+    }
+    if (!rc && level) cudaMemcpy(level, d_lvl, n * sizeof(int32_t), cudaMemcpyDeviceToHost);
+    if (!rc && sigma) cudaMemcpy(sigma, d_sig, n * sizeof(uint64_t), cudaMemcpyDeviceToHost);
+    if (!rc && delta) {
+        cudaMemcpy(delta, d_del, n * sizeof(double), cudaMemcpyDeviceToHost);
+        // unreachable vertices: delta 0
+        if (level)
+            for (size_t v = 0; v < n; ++v) if (level[v] < 0) delta[v] = 0.0;
+    }
+    cudaMemcpy(g->d_bc, d_save, n * sizeof(double), cudaMemcpyDeviceToDevice);
+    cleanup();
+    return rc;
+}
+
+int bcg_graph_pruning(bcg_graph *g, uint32_t *anchor, uint32_t *reach) {
+    clear_error();
+    if (!g) return set_error(BCG_ERR_ARG, "null handle");
+    const size_t n = g->n;
+    if (anchor) {
+        if (g->h_anchor.empty()) for (size_t v = 0; v < n; ++v) anchor[v] = (uint32_t)v;
+        else memcpy(anchor, g->h_anchor.data(), n * sizeof(uint32_t));
+    }
+    if (reach) {
+        if (!g->d_reach) memset(reach, 0, n * sizeof(uint32_t));
+        else CK(cudaMemcpy(reach, g->d_reach, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    }
+    return BCG_OK;
+}
+
+int bcg_graph_info(bcg_graph *g, uint32_t *n, uint64_t *nnz, uint64_t *nnz_pruned, uint32_t *pruned_vertices) {
+    clear_error();
+    if (!g) return set_error(BCG_ERR_ARG, "null handle");
+    if (n) *n = g->n;
+    if (nnz) *nnz = g->nnz;
+    if (nnz_pruned) *nnz_pruned = g->nnz_pruned;
+    if (pruned_vertices) *pruned_vertices = g->npruned;
+    return BCG_OK;
+}
+
+int bcg_graph_set_reach(bcg_graph *g, const uint32_t *reach) {
+    clear_error();
+    if (!g || !reach) return set_error(BCG_ERR_ARG, "null argument");
+    if (g->flags & BCG_PRUNE_DEGREE1) return set_error(BCG_ERR_ARG, "graph was created with BCG_PRUNE_DEGREE1");
+    const size_t n = g->n;
+    std::vector<uint2> vi(n);
+    for (size_t v = 0; v < n; ++v) vi[v] = make_uint2(g->h_deg[v], reach[v]);
+    CK(cudaMemcpy(g->d_vinfo, vi.data(), n * sizeof(uint2), cudaMemcpyHostToDevice));
+    return BCG_OK;
+}
+
+int bcg_run_weighted(bcg_graph *g, const uint32_t *roots, const double *mult, const uint32_t *pend,
+                     uint64_t nroots, bcg_stats *stats) {
+    clear_error();
+    if (!g || (nroots && (!roots || !mult))) return set_error(BCG_ERR_ARG, "null argument");
+    bcg_stats local{};
+    bcg_stats *st = stats ? stats : &local;
+    *st = bcg_stats{};
+    st->sources = nroots;
+    RunPlan p;
+    for (uint64_t i = 0; i < nroots; ++i) {
+        if (roots[i] >= g->n) return set_error(BCG_ERR_ARG, "root %u >= n=%u", roots[i], g->n);
+        p.roots.push_back(roots[i]);
+        p.mult.push_back(mult[i]);
+        p.pend.push_back(pend ? pend[i] : 0u);
+        p.count.push_back(1);
+    }
+    return run_plan(g, p, 0, st, false, nullptr, nullptr);
+}
+
+int bcg_set_batch_width(bcg_graph *g, uint32_t width) {
+    clear_error();
+    if (!g) return set_error(BCG_ERR_ARG, "null handle");
+    if (width != 0 && width != 1 && width != 2 && width != 4 && width != 8)
+        return set_error(BCG_ERR_ARG, "batch width must be 0, 1, 2, 4 or 8");
+    g->forced_width = width;
+    return BCG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,84 @@
+// Device-side definitions shared by the engine's CUDA translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace bcg {
+
+constexpr int kThreads = 512;           // threads per CTA of the sweep kernel
+constexpr int kTileVerts = 512;         // max vertices per tile (one per thread)
+constexpr int kTileEdges = 4096;        // max adjacency entries per tile
+constexpr int kItems = kTileEdges / kThreads;  // edges per thread per tile
+constexpr uint16_t kUnvisited = 0xFFFFu;
+constexpr uint32_t kMaxLevel = 0xFFFDu;  // deepest level a 16-bit row can hold
+constexpr uint32_t kNoRoot = 0xFFFFFFFFu;
+constexpr unsigned long long kDefaultWaitNs = 20ull * 1000 * 1000 * 1000;  // 20 s
+
+// One unit of sweep work: vertices [v0, v1) with all their edges, or one
+// chunk [e0, e1) of the adjacency of a single high-degree vertex (hub >= 0).
+struct Tile {
+    uint32_t v0, v1;
+    uint32_t e0, e1;
+    int32_t hub;       // hub slot, -1 for an ordinary tile
+    uint32_t nchunks;  // chunks of this hub (1 for ordinary tiles)
+    uint32_t pad0, pad1;
+};
+
+// Sweep modes.
+enum : int { kFwdPush = 0, kFwdPull = 1, kBwd = 2 };
+
+// Control block of one kernel launch (zeroed by the host before the launch).
+struct Ctrl {
+    unsigned int bar_count;
+    unsigned int bar_gen;
+    unsigned long long ticket;
+    int error;      // BCG_ERR_* code set by the device, 0 = fine
+    int overflow;   // a uint64 sigma sum wrapped
+    unsigned long long wait_ns;  // bound of every device-side wait
+    // ring of per-sweep counters, indexed by sweep % 4
+    unsigned long long disc[4];  // (vertex, slot) pairs discovered in the sweep
+    unsigned long long pf[4];    // sum of degrees over those pairs
+    // per-slot accumulators of the current batch
+    unsigned long long visited[8];
+    unsigned long long wsum[8];  // sum of (1 + reach) over visited vertices
+    unsigned long long mc2[8];   // sum of (deg + 2 reach) over visited vertices
+    unsigned int depth;
+    unsigned int pad;
+};
+
+// Per-root result of a batch.
+struct RootStat {
+    unsigned long long visited;
+    unsigned long long wsum;
+    unsigned long long mc2;
+    unsigned int depth;
+    unsigned int pad;
+};
+
+struct BatchArgs {
+    uint32_t n;
+    const uint32_t *offs;   // CSR row starts (n+1); pruned lists start here too
+    const uint32_t *adj;    // adjacency (pruned lists compacted to the front)
+    const uint2 *vinfo;     // per vertex {deg in the pruned graph, reach}
+    const Tile *tiles;
+    uint32_t ntiles;
+    uint16_t *lvl;          // n * S levels
+    unsigned long long *val;  // n * S: sigma (forward), then (1+delta)/sigma
+    double *bc;             // n accumulators
+    const uint32_t *roots;  // nbatch * S, kNoRoot = empty slot
+    const double *mult;     // nbatch * S weight of each root's dependencies
+    const uint32_t *pend;   // nbatch * S pendant sources folded into the root
+    uint32_t nbatch;
+    unsigned long long *hub_acc;  // nhub * S
+    unsigned int *hub_cnt;        // nhub
+    Ctrl *ctrl;
+    RootStat *rstat;        // nbatch * S
+    unsigned long long nnz; // adjacency entries of the pruned graph
+    float push_pull_ratio;  // pull when frontier pair-edges >= ratio * unvisited pair-edges
+    int directed;           // 1: adjacency is not symmetric, pull is not allowed
+    // debug outputs for a single-slot single-batch run (nullptr otherwise)
+    unsigned long long *dbg_sigma;
+    double *dbg_delta;
+};
+
+}  // namespace bcg

@@ -1,0 +1,210 @@
+/*
+ * bcg.h — C ABI of the B200 Brandes betweenness-centrality engine (libbcg.so).
+ *
+ * The engine replaces the single-GPU BC path of ck-bc's program/bc-cuda:
+ * the per-source driver loop of bc2d.c (bc2d.c:1016-1050, bc_func_mono
+ * bc2d.c:504-580) and the device state + kernels behind the bc2d.h C ABI
+ * (bc2d.h:132-184, implemented in cuda_kernels.cu).  The reference keeps its
+ * device state in file-static globals and exits on every error
+ * (cudamacro.h:1-16); this ABI is handle based, re-entrant per handle and
+ * returns a status code from every call.  The reference's own mono-path
+ * symbols (initcuda, setcuda, scan_col_csc_cuda_mono, ...) are exported by the
+ * compatibility library described in include/bc2d_compat.h.
+ *
+ * Conventions
+ *   - Graphs are undirected, unweighted, stored as uint32 CSR: offsets[n+1],
+ *     adj[offsets[n]] (the reference's LOCINT = uint32_t CSC, bc2d.h:14,
+ *     build_csc bc2d.c:472-501; for a symmetric graph CSR == CSC).
+ *   - bc values are FP64 sums over ORDERED (source, target) pairs for the
+ *     given source set, i.e. the reference's bc[] before the "/2" it applies
+ *     when writing the result file (bc2d.c:1065).
+ *   - Every function returns BCG_OK (0) or a negative BCG_ERR_* code;
+ *     bcg_last_error() gives a message for the calling thread.
+ */
+#ifndef BCG_H_
+#define BCG_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BCG_OK               0
+#define BCG_ERR_ARG         -1  /* invalid argument (null pointer, id >= n, ...) */
+#define BCG_ERR_CUDA        -2  /* a CUDA runtime call failed */
+#define BCG_ERR_OOM         -3  /* device or host allocation failed / over budget */
+#define BCG_ERR_OVERFLOW    -4  /* a shortest-path count exceeded uint64 */
+#define BCG_ERR_TIMEOUT     -5  /* a device-side bounded wait gave up */
+#define BCG_ERR_IO          -6  /* file could not be opened / parsed */
+#define BCG_ERR_DEPTH       -7  /* BFS deeper than the engine's level limit */
+#define BCG_ERR_RANGE       -8  /* graph too large for 32-bit ids/offsets */
+#define BCG_ERR_NOGPU       -9  /* no CUDA device or kernel image for it */
+
+/* flags for bcg_graph_create */
+#define BCG_PRUNE_DEGREE1   0x1u  /* fold degree-1 vertices into their neighbour (bc2d -H 1) */
+#define BCG_DIRECTED        0x2u  /* adjacency is not symmetric (bc2d -U): traversal follows
+                                     adj[] only; pruning is ignored */
+
+/* ---------------------------------------------------------------------------
+ * Host-side graph ingest and generation (host code, no GPU needed).
+ * ------------------------------------------------------------------------ */
+
+/* Host CSR owned by the library; release with bcg_csr_free. */
+typedef struct bcg_host_csr {
+    uint32_t  n;        /* vertices */
+    uint64_t  nnz;      /* directed adjacency entries = 2 * undirected edges */
+    uint32_t *offsets;  /* n + 1 */
+    uint32_t *adj;      /* nnz, each list sorted ascending, no loops, no duplicates */
+} bcg_host_csr;
+
+/* Reads the reference's edge-list text format (read_graph bc2d.c:175-254):
+ * one "u v" pair per line, 0-based ids < n; any line containing '#' is a
+ * comment ("# Nodes: X Edges: Y" is echoed to stdout when echo_header != 0).
+ * undirected != 0 mirrors every non-loop edge (mirror bc2d.c:152-170, the
+ * default; bc2d -U clears it).  Duplicates and self-loops are dropped
+ * (norm_graph bc2d.c:430-453).  An id >= n fails with BCG_ERR_IO and a message
+ * naming the line, like bc2d.c:232-237. */
+int bcg_csr_read_edgelist(const char *path, uint64_t n, int undirected,
+                          int echo_header, bcg_host_csr *out);
+
+/* Builds a CSR from an explicit edge array (pairs[2*i], pairs[2*i+1]);
+ * same normalisation as bcg_csr_read_edgelist. */
+int bcg_csr_from_pairs(const uint64_t *pairs, uint64_t npairs, uint64_t n,
+                       int undirected, bcg_host_csr *out);
+
+/* Seeded synthetic graphs.  spec is "kind:key=value,..." with kind one of
+ *   rmat  scale, ef, a, b, c, seed [, pendant_frac, pendant_mean, pendant_seed]
+ *   er    scale, ef, seed            (G(n, M) with M = ef * 2^scale draws)
+ *   grid  w, h, drop, seed           (4-neighbour grid, each edge dropped with
+ *                                     probability drop, largest component kept)
+ * The generators and their PRNG (splitmix64) are documented in graph.cpp. */
+int bcg_csr_generate(const char *spec, bcg_host_csr *out);
+
+/* Writes a CSR back as the reference's edge-list text (each undirected edge
+ * once, u < v, with a "# Nodes: N Edges: E" header). */
+int bcg_csr_write_edgelist(const char *path, const bcg_host_csr *g);
+
+void bcg_csr_free(bcg_host_csr *g);
+
+/* k distinct vertices drawn uniformly from [0, n) with the given seed
+ * (partial Fisher-Yates over splitmix64). */
+int bcg_sample_sources(uint32_t n, uint64_t k, uint64_t seed, uint32_t *out);
+
+/* ---------------------------------------------------------------------------
+ * Device engine.
+ * ------------------------------------------------------------------------ */
+
+typedef struct bcg_graph bcg_graph;   /* opaque: one graph resident in HBM */
+
+/* Per-run statistics (all sources of one bcg_run call). */
+typedef struct bcg_stats {
+    uint64_t sources;        /* sources requested */
+    uint64_t skipped;        /* sources with degree 0 (bc2d.c:1026-1034) */
+    uint64_t roots;          /* BFS roots actually run (after pendant folding) */
+    uint64_t batches;        /* multi-source batches launched */
+    uint64_t teps_edges;     /* sum over sources of undirected edges in the
+                                source's connected component (input graph) */
+    uint64_t visited;        /* sum over roots of vertices reached (pruned graph) */
+    uint64_t comp_vertices;  /* sum over sources of the vertex count of the
+                                source's connected component (input graph) */
+    uint32_t max_depth;      /* deepest BFS level seen */
+    uint32_t batch_width;    /* sources per batch (S) */
+    double   kernel_ms;      /* device time of the BC kernels (CUDA events) */
+} bcg_stats;
+
+/* Number of CUDA devices visible (0 when none); never fails. */
+int bcg_device_count(void);
+
+/* Uploads a host CSR to the current device and prepares it (degree-1
+ * pruning when BCG_PRUNE_DEGREE1 is set, work tiles).  offsets/adj are only
+ * read during the call.  Replaces initcuda (cuda_kernels.cu:1123-1198) +
+ * init_bc_1degree/init_bc_1degree_device (bc2d.c:455-465,
+ * cuda_kernels.cu:1083-1087) + degree_reduction (bc2d.c:314-419). */
+int bcg_graph_create(const uint32_t *offsets, const uint32_t *adj, uint32_t n,
+                     uint64_t nnz, uint32_t flags, bcg_graph **out);
+
+/* Same, with offsets/adj already in device memory (copied, not retained). */
+int bcg_graph_create_device(const uint32_t *d_offsets, const uint32_t *d_adj,
+                            uint32_t n, uint64_t nnz, uint32_t flags,
+                            bcg_graph **out);
+
+/* Frees every device buffer of the graph (fincuda cuda_kernels.cu:1201-1232). */
+int bcg_graph_destroy(bcg_graph *g);
+
+/* Sets every bc value of the graph to 0. */
+int bcg_reset_bc(bcg_graph *g);
+
+/* Runs Brandes from every source in sources[0..nsrc) (host array) and ADDS
+ * each source's dependencies into the graph's device bc[] accumulator.
+ * Sources with degree 0 are skipped and counted (bc2d.c:1026-1034).
+ * Replaces the per-source loop bc2d.c:1016-1050 with setcuda/set_mlp_cuda/
+ * scan_col_csc_cuda_mono/scan_frt_csc_cuda_mono/pre_update_bc_cuda/
+ * update_bc_cuda (cuda_kernels.cu:263-336, 689-703, 766-918, 1100-1119). */
+int bcg_run(bcg_graph *g, const uint32_t *sources, uint64_t nsrc,
+            bcg_stats *stats);
+
+/* Same with a device-resident source array; stream is a cudaStream_t (NULL =
+ * legacy default stream).  The source list is read back to the host on that
+ * stream (a stream synchronisation) to fold pendant sources into their
+ * anchors; the BC kernel is then launched on the stream and the call returns
+ * without waiting for it unless stats != NULL. */
+int bcg_run_device(bcg_graph *g, const uint32_t *d_sources, uint64_t nsrc,
+                   void *stream, bcg_stats *stats);
+
+/* Copies the FP64 bc accumulator (n values) to host memory
+ * (get_bc cuda_kernels.cu:1039-1041, which copies float). */
+int bcg_get_bc(bcg_graph *g, double *bc_host);
+
+/* Device pointer of the bc accumulator (n doubles), valid until destroy. */
+int bcg_bc_device_ptr(bcg_graph *g, double **d_bc);
+
+/* One-shot drop-in call on host buffers: upload, run all sources, copy bc
+ * back (bc_out[n], overwritten), free.  flags as bcg_graph_create. */
+int bcg_bc_csr(const uint32_t *offsets, const uint32_t *adj, uint32_t n,
+               uint64_t nnz, const uint32_t *sources, uint64_t nsrc,
+               uint32_t flags, double *bc_out, bcg_stats *stats);
+
+/* Single-source detail for parity checks: BFS depth (-1 = unreachable),
+ * shortest-path count sigma and dependency delta (delta_s(v) =
+ * sum over w with d(w)=d(v)+1 of sigma_v/sigma_w * (1 + delta_w)) of every
+ * vertex, for source src on the graph as created (on the pruned graph when
+ * it was created with BCG_PRUNE_DEGREE1).  Any output pointer may be NULL.
+ * Does not touch the bc accumulator. */
+int bcg_single_source(bcg_graph *g, uint32_t src, int32_t *level,
+                      uint64_t *sigma, double *delta);
+
+/* Pruning result of a graph created with BCG_PRUNE_DEGREE1: anchor[v] = the
+ * vertex v was folded into, or v itself when v was kept; reach[v] = number of
+ * vertices folded into v.  Either pointer may be NULL. */
+int bcg_graph_pruning(bcg_graph *g, uint32_t *anchor, uint32_t *reach);
+
+/* Graph sizes after preparation. */
+int bcg_graph_info(bcg_graph *g, uint32_t *n, uint64_t *nnz,
+                   uint64_t *nnz_pruned, uint32_t *pruned_vertices);
+
+/* Sets per-vertex pendant weights computed by the caller (the reference's
+ * reach[] from its host-side degree_reduction, bc2d.c:314-419 + 455-465,
+ * handed over by init_bc_1degree_device, cuda_kernels.cu:1083-1087).  Only
+ * for graphs created without BCG_PRUNE_DEGREE1. */
+int bcg_graph_set_reach(bcg_graph *g, const uint32_t *reach);
+
+/* Runs explicit BFS roots with explicit weights: root k's dependencies are
+ * added mult[k] times and bc[root] += pend[k] * (W - 2), W = sum over the
+ * root's component of (1 + reach) (update_bc cuda_kernels.cu:263-277 with
+ * reach_v0: mult = reach_v0 + 1, pend = reach_v0).  No degree-0 skip and no
+ * pendant folding.  pend may be NULL (all 0). */
+int bcg_run_weighted(bcg_graph *g, const uint32_t *roots, const double *mult,
+                     const uint32_t *pend, uint64_t nroots, bcg_stats *stats);
+
+/* Forces the sources-per-batch width (1, 2, 4 or 8; 0 = automatic). */
+int bcg_set_batch_width(bcg_graph *g, uint32_t width);
+
+/* Message for the last error of the calling thread ("" if none). */
+const char *bcg_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BCG_H_ */
