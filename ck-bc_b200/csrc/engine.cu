@@ -117,14 +117,19 @@ __global__ void k_levels_out(uint32_t n, const uint16_t *__restrict__ lvl, int32
 // Work tiles (host, from the original row starts).
 // ---------------------------------------------------------------------------
 
-static void build_tiles(const uint32_t *offs, uint32_t n, std::vector<Tile> &tiles, uint32_t &nhub) {
+// tile_of[v] = index of v's tile (of its first chunk, with kHubFlag, when v
+// is split).
+static void build_tiles(const uint32_t *offs, uint32_t n, std::vector<Tile> &tiles, uint32_t &nhub,
+                        std::vector<uint32_t> &tile_of) {
     tiles.clear();
+    tile_of.assign(n, 0);
     nhub = 0;
     uint32_t v = 0;
     while (v < n) {
         const uint32_t dv = offs[v + 1] - offs[v];
         if (dv > (uint32_t)kTileEdges) {
             const uint32_t nch = (dv + kTileEdges - 1) / kTileEdges;
+            tile_of[v] = (uint32_t)tiles.size() | kHubFlag;
             for (uint32_t c = 0; c < nch; ++c) {
                 Tile t{};
                 t.v0 = v; t.v1 = v + 1;
@@ -144,6 +149,7 @@ static void build_tiles(const uint32_t *offs, uint32_t n, std::vector<Tile> &til
             const uint32_t d = offs[v + 1] - offs[v];
             if (d > (uint32_t)kTileEdges || sum + d > (uint32_t)kTileEdges) break;
             sum += d;
+            tile_of[v] = (uint32_t)tiles.size();
             ++v;
         }
         Tile t{};
@@ -173,6 +179,10 @@ struct bcg_graph {
     uint32_t ntiles = 0, nhub = 0;
     unsigned long long *d_hub_acc = nullptr;
     unsigned int *d_hub_cnt = nullptr;
+    uint32_t *d_tile_of = nullptr, *d_tmark = nullptr;
+    uint32_t *d_lists = nullptr, *d_lbase = nullptr, *d_lcnt = nullptr;
+    uint32_t *d_ulist = nullptr;  // ring of 2 * ntiles (tiles with unvisited vertices)
+    unsigned long long list_cap = 0;
     uint16_t *d_lvl = nullptr;
     unsigned long long *d_val = nullptr;
     uint32_t state_width = 0;
@@ -199,6 +209,8 @@ static void graph_free(bcg_graph *g) {
     cudaFree(g->d_offs); cudaFree(g->d_adj); cudaFree(g->d_vinfo);
     cudaFree(g->d_anchor); cudaFree(g->d_reach); cudaFree(g->d_bc);
     cudaFree(g->d_tiles); cudaFree(g->d_hub_acc); cudaFree(g->d_hub_cnt);
+    cudaFree(g->d_tile_of); cudaFree(g->d_tmark); cudaFree(g->d_lists);
+    cudaFree(g->d_lbase); cudaFree(g->d_lcnt); cudaFree(g->d_ulist);
     cudaFree(g->d_lvl); cudaFree(g->d_val); cudaFree(g->d_ctrl);
     cudaFree(g->d_roots); cudaFree(g->d_pend); cudaFree(g->d_mult); cudaFree(g->d_rstat);
     if (g->ev0) cudaEventDestroy(g->ev0);
@@ -212,11 +224,18 @@ static int ensure_state(bcg_graph *g, uint32_t S) {
     cudaFree(g->d_lvl); g->d_lvl = nullptr;
     cudaFree(g->d_val); g->d_val = nullptr;
     cudaFree(g->d_hub_acc); g->d_hub_acc = nullptr;
+    cudaFree(g->d_lists); g->d_lists = nullptr;
     g->state_width = 0;
     CK(cudaMalloc(&g->d_lvl, (size_t)g->n * S * sizeof(uint16_t)));
-    CK(cudaMalloc(&g->d_val, (size_t)g->n * S * sizeof(unsigned long long)));
+    // three value arrays (levels mod 3), n * S each
+    CK(cudaMalloc(&g->d_val, 3 * (size_t)g->n * S * sizeof(unsigned long long)));
     CK(cudaMalloc(&g->d_hub_acc, (size_t)std::max(1u, g->nhub) * S * sizeof(unsigned long long)));
     CK(cudaMemset(g->d_hub_acc, 0, (size_t)std::max(1u, g->nhub) * S * sizeof(unsigned long long)));
+    // every (tile, level) pair is listed at most once per batch: a tile is on
+    // level d's list only if one of its vertices (or chunks) first reaches d,
+    // so the lists of one batch hold at most S * (n + ntiles) entries
+    g->list_cap = (unsigned long long)S * ((unsigned long long)g->n + g->ntiles);
+    CK(cudaMalloc(&g->d_lists, g->list_cap * sizeof(uint32_t)));
     g->state_width = S;
     return BCG_OK;
 }
@@ -236,10 +255,10 @@ static int ensure_run(bcg_graph *g, size_t slots) {
 }
 
 // Sources per batch: the widest S in {8,4,2,1} whose per-vertex state
-// (S * (2 + 8) bytes) fits the L2-resident budget, and not wider than needed.
+// (S * (2 + 8) bytes) fits the state budget, and not wider than needed.
 static uint32_t choose_width(const bcg_graph *g, uint64_t nroots) {
     if (g->forced_width) return g->forced_width;
-    double budget = 56.0 * 1024 * 1024;
+    double budget = 160.0 * 1024 * 1024;
     if (const char *e = getenv("BCG_STATE_BUDGET_MB")) budget = atof(e) * 1024 * 1024;
     uint32_t S = 8;
     while (S > 1 && (double)g->n * S * 10.0 > budget) S >>= 1;
@@ -281,11 +300,18 @@ static int create_common(bcg_graph *g, const uint32_t *h_offs) {
         g->nnz_pruned = g->nnz;
     }
     std::vector<Tile> tiles;
-    build_tiles(h_offs, n, tiles, g->nhub);
+    std::vector<uint32_t> tile_of;
+    build_tiles(h_offs, n, tiles, g->nhub, tile_of);
     g->ntiles = (uint32_t)tiles.size();
     CK(cudaMalloc(&g->d_tiles, std::max<size_t>(1, tiles.size()) * sizeof(Tile)));
     if (!tiles.empty())
         CK(cudaMemcpy(g->d_tiles, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&g->d_tile_of, (size_t)n * sizeof(uint32_t)));
+    CK(cudaMemcpy(g->d_tile_of, tile_of.data(), (size_t)n * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&g->d_tmark, std::max<size_t>(1, tiles.size()) * sizeof(uint32_t)));
+    CK(cudaMalloc(&g->d_lbase, (size_t)(kMaxLevel + 3) * sizeof(uint32_t)));
+    CK(cudaMalloc(&g->d_lcnt, (size_t)(kMaxLevel + 3) * sizeof(uint32_t)));
+    CK(cudaMalloc(&g->d_ulist, 2 * std::max<size_t>(1, tiles.size()) * sizeof(uint32_t)));
     CK(cudaMalloc(&g->d_hub_cnt, (size_t)std::max(1u, g->nhub) * sizeof(unsigned int)));
     CK(cudaMemset(g->d_hub_cnt, 0, (size_t)std::max(1u, g->nhub) * sizeof(unsigned int)));
     CK(cudaDeviceSynchronize());
@@ -364,10 +390,8 @@ static int run_plan(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *
     CK(cudaMemcpyAsync(g->d_roots, roots.data(), slots * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(g->d_pend, pend.data(), slots * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(g->d_mult, mult.data(), slots * sizeof(double), cudaMemcpyHostToDevice, st));
-    CK(cudaMemsetAsync(g->d_ctrl, 0, sizeof(Ctrl), st));
     CK(cudaMemsetAsync(g->d_hub_acc, 0, (size_t)std::max(1u, g->nhub) * g->state_width * sizeof(unsigned long long), st));
     CK(cudaMemsetAsync(g->d_hub_cnt, 0, (size_t)std::max(1u, g->nhub) * sizeof(unsigned int), st));
-    CK(cudaMemcpyAsync(&g->d_ctrl->wait_ns, &g->wait_ns, sizeof(unsigned long long), cudaMemcpyHostToDevice, st));
     BatchArgs a{};
     a.n = g->n;
     a.offs = g->d_offs;
@@ -375,27 +399,79 @@ static int run_plan(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *
     a.vinfo = g->d_vinfo;
     a.tiles = g->d_tiles;
     a.ntiles = g->ntiles;
+    a.tile_of = g->d_tile_of;
+    a.tmark = g->d_tmark;
+    a.lists = g->d_lists;
+    a.list_cap = g->list_cap;
+    a.ulist = g->d_ulist;
+    a.lbase = g->d_lbase;
+    a.lcnt = g->d_lcnt;
     a.lvl = g->d_lvl;
     a.val = g->d_val;
     a.bc = g->d_bc;
-    a.roots = g->d_roots;
-    a.mult = g->d_mult;
-    a.pend = g->d_pend;
-    a.nbatch = (uint32_t)nbatch;
     a.hub_acc = g->d_hub_acc;
     a.hub_cnt = g->d_hub_cnt;
     a.ctrl = g->d_ctrl;
-    a.rstat = g->d_rstat;
     a.nnz = g->nnz_pruned;
     a.push_pull_ratio = g->ratio;
     a.directed = (g->flags & BCG_DIRECTED) ? 1 : 0;
     a.dbg_sigma = dbg_sigma;
     a.dbg_delta = dbg_delta;
+    // optional per-sweep trace: BCG_TRACE_FILE=<path> appends one CSV line per
+    // sweep (batch, kind, level, tiles walked, pairs discovered, end time)
+    const char *trace_path = getenv("BCG_TRACE_FILE");
+    TraceRec *d_trace = nullptr;
+    unsigned int *d_tcnt = nullptr;
+    const unsigned int trace_cap = 1u << 20;
+    if (trace_path && *trace_path) {
+        CK(cudaMalloc(&d_trace, trace_cap * sizeof(TraceRec)));
+        CK(cudaMalloc(&d_tcnt, sizeof(unsigned int)));
+        CK(cudaMemsetAsync(d_tcnt, 0, sizeof(unsigned int), st));
+        a.trace = d_trace;
+        a.trace_cap = trace_cap;
+        a.trace_cnt = d_tcnt;
+    }
     CK(cudaEventRecord(g->ev0, st));
-    int grid = 0;
-    rc = launch_sweep((int)S, a, st, &grid);
-    if (rc) return rc;
+    // tile marks key on the batch index modulo 2^16, so one launch runs at most
+    // 65535 batches and the marks are cleared before every launch
+    const uint64_t per_launch = 65535;
+    for (uint64_t b0 = 0; b0 < nbatch; b0 += per_launch) {
+        const uint64_t nb = std::min(per_launch, nbatch - b0);
+        CK(cudaMemsetAsync(g->d_ctrl, 0, sizeof(Ctrl), st));
+        CK(cudaMemcpyAsync(&g->d_ctrl->wait_ns, &g->wait_ns, sizeof(unsigned long long), cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(g->d_tmark, 0, (size_t)std::max(1u, g->ntiles) * sizeof(uint32_t), st));
+        a.roots = g->d_roots + b0 * S;
+        a.mult = g->d_mult + b0 * S;
+        a.pend = g->d_pend + b0 * S;
+        a.rstat = g->d_rstat + b0 * S;
+        a.nbatch = (uint32_t)nb;
+        int grid = 0;
+        rc = launch_sweep((int)S, a, st, &grid);
+        if (rc) return rc;
+        if (b0 + nb < nbatch) {
+            // errors of this launch are read before the control block is reused
+            CK(cudaStreamSynchronize(st));
+            Ctrl c{};
+            CK(cudaMemcpy(&c, g->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+            if (c.error || c.overflow) break;
+        }
+    }
     CK(cudaEventRecord(g->ev1, st));
+    if (d_trace) {
+        CK(cudaStreamSynchronize(st));
+        unsigned int cnt = 0;
+        CK(cudaMemcpy(&cnt, d_tcnt, sizeof(cnt), cudaMemcpyDeviceToHost));
+        std::vector<TraceRec> recs(cnt);
+        if (cnt) CK(cudaMemcpy(recs.data(), d_trace, cnt * sizeof(TraceRec), cudaMemcpyDeviceToHost));
+        cudaFree(d_trace);
+        cudaFree(d_tcnt);
+        if (FILE *f = fopen(trace_path, "a")) {
+            fprintf(f, "# width %u roots %zu tiles %u\n", S, (size_t)nroots, g->ntiles);
+            for (const TraceRec &r : recs)
+                fprintf(f, "%u,%u,%u,%u,%llu,%llu\n", r.batch, r.kind, r.level, r.nwork, r.disc, r.t_ns);
+            fclose(f);
+        }
+    }
     if (!stats && !debug) return BCG_OK;
     CK(cudaStreamSynchronize(st));
     Ctrl c{};

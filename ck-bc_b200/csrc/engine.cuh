@@ -5,13 +5,17 @@
 
 namespace bcg {
 
-constexpr int kThreads = 512;           // threads per CTA of the sweep kernel
-constexpr int kTileVerts = 512;         // max vertices per tile (one per thread)
-constexpr int kTileEdges = 4096;        // max adjacency entries per tile
-constexpr int kItems = kTileEdges / kThreads;  // edges per thread per tile
+constexpr int kThreads = 512;            // threads per CTA of the sweep kernel
+constexpr int kWarps = kThreads / 32;    // independent tile workers per CTA
+constexpr int kTileVerts = 32;           // max vertices per tile (one per lane)
+constexpr int kTileEdges = 256;          // max adjacency entries per tile
+constexpr int kItems = kTileEdges / 32;  // edges per lane per tile
+constexpr int kSub = 4;                  // edges per lane in flight at once
 constexpr uint16_t kUnvisited = 0xFFFFu;
 constexpr uint32_t kMaxLevel = 0xFFFDu;  // deepest level a 16-bit row can hold
 constexpr uint32_t kNoRoot = 0xFFFFFFFFu;
+constexpr uint32_t kNoTile = 0xFFFFFFFFu;
+constexpr uint32_t kHubFlag = 0x80000000u;  // tile_of[v] flag: v is split into chunks
 constexpr unsigned long long kDefaultWaitNs = 20ull * 1000 * 1000 * 1000;  // 20 s
 
 // One unit of sweep work: vertices [v0, v1) with all their edges, or one
@@ -31,10 +35,10 @@ enum : int { kFwdPush = 0, kFwdPull = 1, kBwd = 2 };
 struct Ctrl {
     unsigned int bar_count;
     unsigned int bar_gen;
-    unsigned long long ticket;
     int error;      // BCG_ERR_* code set by the device, 0 = fine
     int overflow;   // a uint64 sigma sum wrapped
     unsigned long long wait_ns;  // bound of every device-side wait
+    unsigned long long uctr;     // monotone write position in the unvisited-tile ring
     // ring of per-sweep counters, indexed by sweep % 4
     unsigned long long disc[4];  // (vertex, slot) pairs discovered in the sweep
     unsigned long long pf[4];    // sum of degrees over those pairs
@@ -42,8 +46,17 @@ struct Ctrl {
     unsigned long long visited[8];
     unsigned long long wsum[8];  // sum of (1 + reach) over visited vertices
     unsigned long long mc2[8];   // sum of (deg + 2 reach) over visited vertices
-    unsigned int depth;
-    unsigned int pad;
+};
+
+// One record of the optional sweep trace (written by CTA 0 after each grid
+// barrier when BatchArgs::trace is set).
+struct TraceRec {
+    unsigned long long t_ns;   // %globaltimer when the phase ended
+    unsigned int batch;
+    unsigned int kind;         // 0 init, 1 push, 2 pull, 3 backward, 4 batch end
+    unsigned int level;
+    unsigned int nwork;        // tiles walked
+    unsigned long long disc;   // (vertex, slot) pairs discovered (forward)
 };
 
 // Per-root result of a batch.
@@ -62,8 +75,18 @@ struct BatchArgs {
     const uint2 *vinfo;     // per vertex {deg in the pruned graph, reach}
     const Tile *tiles;
     uint32_t ntiles;
+    const uint32_t *tile_of;  // per vertex: its tile (first chunk | kHubFlag for hubs)
+    uint32_t *tmark;        // per tile: (batch, level) key of its last list append
+    uint32_t *lists;        // per-level lists of active tiles, back to back
+    unsigned long long list_cap;
+    uint32_t *lbase;        // kMaxLevel + 3: start of level d's list
+    uint32_t *lcnt;         // kMaxLevel + 3: length of level d's list
+    uint32_t *ulist;        // ring of 2 * ntiles: tiles that still hold unvisited vertices
     uint16_t *lvl;          // n * S levels
-    unsigned long long *val;  // n * S: sigma (forward), then (1+delta)/sigma
+    // 3 * n * S values: the value of (v, slot k) at level L lives in array
+    // L mod 3, val[((L % 3) * n + v) * S + k]: sigma in the forward pass,
+    // (1 + delta) / sigma after v's backward step; the other two arrays hold 0
+    unsigned long long *val;
     double *bc;             // n accumulators
     const uint32_t *roots;  // nbatch * S, kNoRoot = empty slot
     const double *mult;     // nbatch * S weight of each root's dependencies
@@ -79,6 +102,10 @@ struct BatchArgs {
     // debug outputs for a single-slot single-batch run (nullptr otherwise)
     unsigned long long *dbg_sigma;
     double *dbg_delta;
+    // optional sweep trace (nullptr = off); trace_cnt counts records written
+    TraceRec *trace;
+    unsigned int trace_cap;
+    unsigned int *trace_cnt;
 };
 
 }  // namespace bcg
