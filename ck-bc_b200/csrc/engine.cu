@@ -108,9 +108,12 @@ __global__ void k_vinfo_plain(uint32_t n, const uint32_t *__restrict__ offs, uin
     if (v < n) vinfo[v] = make_uint2(offs[v + 1] - offs[v], 0u);
 }
 
-__global__ void k_levels_out(uint32_t n, const uint16_t *__restrict__ lvl, int32_t *__restrict__ out) {
+// Levels of slot 0 of a single-slot run (rows of row_bytes(1) bytes, level first).
+__global__ void k_levels_out(uint32_t n, const unsigned char *__restrict__ rows, int32_t *__restrict__ out) {
     const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v < n) out[v] = lvl[v] == kUnvisited ? -1 : (int32_t)lvl[v];
+    if (v >= n) return;
+    const uint16_t l = *reinterpret_cast<const uint16_t *>(rows + (size_t)v * row_bytes(1));
+    out[v] = l == kUnvisited ? -1 : (int32_t)l;
 }
 
 // ---------------------------------------------------------------------------
@@ -183,8 +186,7 @@ struct bcg_graph {
     uint32_t *d_lists = nullptr, *d_lbase = nullptr, *d_lcnt = nullptr;
     uint32_t *d_ulist = nullptr;  // ring of 2 * ntiles (tiles with unvisited vertices)
     unsigned long long list_cap = 0;
-    uint16_t *d_lvl = nullptr;
-    unsigned long long *d_val = nullptr;
+    unsigned char *d_rows = nullptr;  // n state rows of row_bytes(state_width)
     uint32_t state_width = 0;
     Ctrl *d_ctrl = nullptr;
     uint32_t *d_roots = nullptr, *d_pend = nullptr;
@@ -211,7 +213,7 @@ static void graph_free(bcg_graph *g) {
     cudaFree(g->d_tiles); cudaFree(g->d_hub_acc); cudaFree(g->d_hub_cnt);
     cudaFree(g->d_tile_of); cudaFree(g->d_tmark); cudaFree(g->d_lists);
     cudaFree(g->d_lbase); cudaFree(g->d_lcnt); cudaFree(g->d_ulist);
-    cudaFree(g->d_lvl); cudaFree(g->d_val); cudaFree(g->d_ctrl);
+    cudaFree(g->d_rows); cudaFree(g->d_ctrl);
     cudaFree(g->d_roots); cudaFree(g->d_pend); cudaFree(g->d_mult); cudaFree(g->d_rstat);
     if (g->ev0) cudaEventDestroy(g->ev0);
     if (g->ev1) cudaEventDestroy(g->ev1);
@@ -220,15 +222,12 @@ static void graph_free(bcg_graph *g) {
 }
 
 static int ensure_state(bcg_graph *g, uint32_t S) {
-    if (g->state_width >= S) return BCG_OK;
-    cudaFree(g->d_lvl); g->d_lvl = nullptr;
-    cudaFree(g->d_val); g->d_val = nullptr;
+    if (g->state_width >= S) return BCG_OK;  // row_bytes grows with S
+    cudaFree(g->d_rows); g->d_rows = nullptr;
     cudaFree(g->d_hub_acc); g->d_hub_acc = nullptr;
     cudaFree(g->d_lists); g->d_lists = nullptr;
     g->state_width = 0;
-    CK(cudaMalloc(&g->d_lvl, (size_t)g->n * S * sizeof(uint16_t)));
-    // three value arrays (levels mod 3), n * S each
-    CK(cudaMalloc(&g->d_val, 3 * (size_t)g->n * S * sizeof(unsigned long long)));
+    CK(cudaMalloc(&g->d_rows, (size_t)g->n * row_bytes((int)S)));
     CK(cudaMalloc(&g->d_hub_acc, (size_t)std::max(1u, g->nhub) * S * sizeof(unsigned long long)));
     CK(cudaMemset(g->d_hub_acc, 0, (size_t)std::max(1u, g->nhub) * S * sizeof(unsigned long long)));
     // every (tile, level) pair is listed at most once per batch: a tile is on
@@ -254,15 +253,16 @@ static int ensure_run(bcg_graph *g, size_t slots) {
     return BCG_OK;
 }
 
-// Sources per batch: the widest S in {8,4,2,1} whose per-vertex state
-// (S * (2 + 8) bytes) fits the state budget, and not wider than needed.
+// Sources per batch: the widest S in {6, 3, 1} whose state rows
+// (n * row_bytes(S)) fit the budget that keeps them L2-resident, and not
+// wider than the number of roots needs.
 static uint32_t choose_width(const bcg_graph *g, uint64_t nroots) {
     if (g->forced_width) return g->forced_width;
-    double budget = 160.0 * 1024 * 1024;
+    double budget = 64.0 * 1024 * 1024;
     if (const char *e = getenv("BCG_STATE_BUDGET_MB")) budget = atof(e) * 1024 * 1024;
-    uint32_t S = 8;
-    while (S > 1 && (double)g->n * S * 10.0 > budget) S >>= 1;
-    while (S > 1 && (uint64_t)(S >> 1) >= nroots) S >>= 1;
+    uint32_t S = 6;
+    if ((double)g->n * row_bytes(6) > budget || nroots <= 3) S = 3;
+    if (S == 3 && ((double)g->n * row_bytes(3) > budget || nroots <= 1)) S = 1;
     return S;
 }
 
@@ -406,8 +406,7 @@ static int run_plan(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *
     a.ulist = g->d_ulist;
     a.lbase = g->d_lbase;
     a.lcnt = g->d_lcnt;
-    a.lvl = g->d_lvl;
-    a.val = g->d_val;
+    a.rows = g->d_rows;
     a.bc = g->d_bc;
     a.hub_acc = g->d_hub_acc;
     a.hub_cnt = g->d_hub_cnt;
@@ -548,11 +547,14 @@ static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint3
     auto fail = [&](int code) { graph_free(g); return code; };
     cudaError_t e;
     if ((e = cudaMalloc(&g->d_offs, ((size_t)n + 1) * sizeof(uint32_t))) != cudaSuccess ||
-        (e = cudaMalloc(&g->d_adj, std::max<uint64_t>(nnz, 1) * sizeof(uint32_t))) != cudaSuccess)
+        // 4 entries of tail padding: the sweep copies adjacency ranges in
+        // 16-byte aligned chunks that may end up to 12 bytes past nnz
+        (e = cudaMalloc(&g->d_adj, (nnz + 4) * sizeof(uint32_t))) != cudaSuccess)
         return fail(set_error(BCG_ERR_OOM, "cudaMalloc CSR: %s", cudaGetErrorString(e)));
     const cudaMemcpyKind kind = device_in ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     if ((e = cudaMemcpy(g->d_offs, offsets, ((size_t)n + 1) * sizeof(uint32_t), kind)) != cudaSuccess ||
-        (nnz && (e = cudaMemcpy(g->d_adj, adj, nnz * sizeof(uint32_t), kind)) != cudaSuccess))
+        (nnz && (e = cudaMemcpy(g->d_adj, adj, nnz * sizeof(uint32_t), kind)) != cudaSuccess) ||
+        (e = cudaMemset(g->d_adj + nnz, 0, 4 * sizeof(uint32_t))) != cudaSuccess)
         return fail(set_error(BCG_ERR_CUDA, "uploading CSR: %s", cudaGetErrorString(e)));
     rc = create_common(g, ho);
     if (rc) return fail(rc);
@@ -669,7 +671,7 @@ int bcg_single_source(bcg_graph *g, uint32_t src, int32_t *level, uint64_t *sigm
     p.count.push_back(1);
     rc = run_plan(g, p, 0, nullptr, true, d_sig, d_del);
     if (!rc) {
-        k_levels_out<<<(unsigned)((n + 255) / 256), 256>>>(g->n, g->d_lvl, d_lvl);
+        k_levels_out<<<(unsigned)((n + 255) / 256), 256>>>(g->n, g->d_rows, d_lvl);
         cudaError_t e = cudaDeviceSynchronize();
         if (e != cudaSuccess) rc = set_error(BCG_ERR_CUDA, "levels: %s", cudaGetErrorString(e));
     }
@@ -744,8 +746,8 @@ int bcg_run_weighted(bcg_graph *g, const uint32_t *roots, const double *mult, co
 int bcg_set_batch_width(bcg_graph *g, uint32_t width) {
     clear_error();
     if (!g) return set_error(BCG_ERR_ARG, "null handle");
-    if (width != 0 && width != 1 && width != 2 && width != 4 && width != 8)
-        return set_error(BCG_ERR_ARG, "batch width must be 0, 1, 2, 4 or 8");
+    if (width != 0 && width != 1 && width != 3 && width != 6)
+        return set_error(BCG_ERR_ARG, "batch width must be 0, 1, 3 or 6");
     g->forced_width = width;
     return BCG_OK;
 }

@@ -10,13 +10,31 @@ constexpr int kWarps = kThreads / 32;    // independent tile workers per CTA
 constexpr int kTileVerts = 32;           // max vertices per tile (one per lane)
 constexpr int kTileEdges = 256;          // max adjacency entries per tile
 constexpr int kItems = kTileEdges / 32;  // edges per lane per tile
-constexpr int kSub = 4;                  // edges per lane in flight at once
+constexpr int kStageBytes = 8192;        // per-warp shared staging of gathered rows
+constexpr int kPushSplit = 8;            // sparse push sweeps: warps per tile
 constexpr uint16_t kUnvisited = 0xFFFFu;
-constexpr uint32_t kMaxLevel = 0xFFFDu;  // deepest level a 16-bit row can hold
+constexpr uint32_t kMaxLevel = 0xFFFDu;  // deepest level a 16-bit level can hold
 constexpr uint32_t kNoRoot = 0xFFFFFFFFu;
 constexpr uint32_t kNoTile = 0xFFFFFFFFu;
 constexpr uint32_t kHubFlag = 0x80000000u;  // tile_of[v] flag: v is split into chunks
 constexpr unsigned long long kDefaultWaitNs = 20ull * 1000 * 1000 * 1000;  // 20 s
+
+// Per-vertex state row of a batch of S slots (S in {1, 3, 6}): a level block
+// of S 16-bit levels padded to 8 bytes (16 for S = 6), then S 64-bit values:
+// 16, 32 or 64 bytes, i.e. half of, one or two 32-byte sectors.  The value of
+// a slot is sigma during the forward pass and (1 + delta) / sigma after the
+// vertex's backward step.
+template <int S>
+struct RowGeom {
+    static_assert(S == 1 || S == 3 || S == 6, "batch width must be 1, 3 or 6");
+    static constexpr int kLvlBytes = (S <= 4) ? 8 : 16;
+    static constexpr int kBytes = kLvlBytes + 8 * S;
+    static constexpr int kWords = kBytes / 4;
+    static constexpr int kVec = kBytes / 16;
+    static constexpr int kValWord = kLvlBytes / 4;  // first word of the values
+};
+
+__host__ __device__ constexpr int row_bytes(int S) { return ((S <= 4) ? 8 : 16) + 8 * S; }
 
 // One unit of sweep work: vertices [v0, v1) with all their edges, or one
 // chunk [e0, e1) of the adjacency of a single high-degree vertex (hub >= 0).
@@ -53,7 +71,7 @@ struct Ctrl {
 struct TraceRec {
     unsigned long long t_ns;   // %globaltimer when the phase ended
     unsigned int batch;
-    unsigned int kind;         // 0 init, 1 push, 2 pull, 3 backward, 4 batch end
+    unsigned int kind;         // 0 init, 1 push, 2 pull, 3 backward
     unsigned int level;
     unsigned int nwork;        // tiles walked
     unsigned long long disc;   // (vertex, slot) pairs discovered (forward)
@@ -82,11 +100,7 @@ struct BatchArgs {
     uint32_t *lbase;        // kMaxLevel + 3: start of level d's list
     uint32_t *lcnt;         // kMaxLevel + 3: length of level d's list
     uint32_t *ulist;        // ring of 2 * ntiles: tiles that still hold unvisited vertices
-    uint16_t *lvl;          // n * S levels
-    // 3 * n * S values: the value of (v, slot k) at level L lives in array
-    // L mod 3, val[((L % 3) * n + v) * S + k]: sigma in the forward pass,
-    // (1 + delta) / sigma after v's backward step; the other two arrays hold 0
-    unsigned long long *val;
+    unsigned char *rows;    // n state rows of row_bytes(S)
     double *bc;             // n accumulators
     const uint32_t *roots;  // nbatch * S, kNoRoot = empty slot
     const double *mult;     // nbatch * S weight of each root's dependencies

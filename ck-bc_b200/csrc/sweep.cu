@@ -21,26 +21,26 @@
 // Grid-wide barriers between sweeps are software barriers whose waits give up
 // after Ctrl::wait_ns, set an error code and let every CTA return.
 //
-// Values rotate over three arrays by level mod 3.  The neighbours of a vertex
-// at level L sit at levels L-1, L and L+1 only, so in the array of level L+1
-// the only non-zero entries a level-L vertex can see are its children's, and
-// in the array of level L the only non-zero entries an unvisited vertex can
-// see during the level-L pull are its parents'.  Pull and backward sweeps
-// therefore sum the neighbour's whole value row without reading its levels:
-// one gather of S*8 bytes per edge for all S slots.  Push sweeps read the
-// neighbour's 16-bit level row to claim it.
+// State.  One row per vertex holds the S levels and the S values (RowGeom):
+// a 32-byte row for S = 3, so one gathered sector answers both "is this
+// neighbour at the wanted level" and "what is its value" for all slots.  With
+// S = 3 the rows of a 1.5M-vertex graph take 47 MB and stay in the 126 MB L2
+// while the adjacency streams past with an evict-first policy.
 //
 // Work decomposition.  Vertices are cut into static tiles of <= 32
 // consecutive vertices and <= 256 adjacency entries; a vertex with more than
 // 256 neighbours is split into 256-entry chunks whose partial sums meet in
-// hub_acc (the last chunk to arrive finishes the vertex).  Every warp works
-// on one tile at a time with no CTA-wide synchronisation: lane j owns vertex j
-// of the tile, the tile's edges are cut into contiguous runs of 8 per lane
-// (merge-path over the warp's exclusive scan of active degrees).
-// Push and backward sweeps walk only the tiles on the level's list (tiles
-// holding a vertex first reached at that level, for any slot); pull sweeps walk
-// the tiles that still hold an unvisited vertex (all tiles in the first pull of
-// a batch).  Both lists are written through warp-buffered appends.
+// hub_acc (the last chunk to arrive finishes the vertex).  One warp works on
+// one tile at a time with no CTA-wide synchronisation: lane j owns vertex j,
+// the tile's edges are cut into contiguous runs of <= 8 per lane (merge-path
+// over the warp's exclusive scan of active degrees).  Each lane loads its
+// run's adjacency entries, then issues cp.async copies of all their rows into
+// its slice of the warp's shared staging buffer, so a tile costs two dependent
+// global round trips however many edges are in flight.  Push and backward
+// sweeps walk only the tiles on the level's list (tiles holding a vertex first
+// reached at that level, for any slot; a sparse push splits each tile over
+// kPushSplit warps); pull sweeps walk the tiles that still hold an unvisited
+// vertex (all tiles in the first pull of a batch).
 #include <cstdio>
 
 #include "bcg.h"
@@ -63,18 +63,30 @@ __device__ __forceinline__ uint32_t vload32(const uint32_t *p) {
     return *reinterpret_cast<const volatile uint32_t *>(p);
 }
 
-// L2 policy for streamed data: evicted before the per-vertex rows.
+// L2 policy for streamed data: evicted before the state rows.
 __device__ __forceinline__ unsigned long long evict_first_policy() {
     unsigned long long pol;
     asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
     return pol;
 }
 
-// Streaming read of the adjacency (read-only for the whole launch).
-__device__ __forceinline__ uint32_t ld_adj(const uint32_t *p, unsigned long long pol) {
-    uint32_t v;
-    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
-    return v;
+// Asynchronous global -> shared copies (completion: cp_wait_all).
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+}
+// 16-byte copy of streamed data (L2 only, evict-first policy).
+__device__ __forceinline__ void cp_async16_stream(void *smem, const void *gmem, unsigned long long pol) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(s), "l"(gmem), "l"(pol)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_wait_all() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
 
 // Software grid barrier (all CTAs co-resident: cooperative launch).  Returns
@@ -110,62 +122,34 @@ __device__ bool grid_sync(Ctrl *c, unsigned int nblocks, unsigned long long wait
     return *reinterpret_cast<volatile int *>(&c->error) == 0;
 }
 
-template <int S>
-__device__ __forceinline__ void load_row(const uint16_t *base, uint32_t v, uint16_t (&r)[S]) {
-    const uint16_t *p = base + (size_t)v * S;
-    if constexpr (S == 1) {
-        r[0] = p[0];
-    } else if constexpr (S == 2) {
-        uint32_t x = *reinterpret_cast<const uint32_t *>(p);
-        r[0] = (uint16_t)x;
-        r[1] = (uint16_t)(x >> 16);
-    } else if constexpr (S == 4) {
-        uint2 x = *reinterpret_cast<const uint2 *>(p);
-        r[0] = (uint16_t)x.x; r[1] = (uint16_t)(x.x >> 16);
-        r[2] = (uint16_t)x.y; r[3] = (uint16_t)(x.y >> 16);
-    } else {
-        uint4 x = *reinterpret_cast<const uint4 *>(p);
-        r[0] = (uint16_t)x.x; r[1] = (uint16_t)(x.x >> 16);
-        r[2] = (uint16_t)x.y; r[3] = (uint16_t)(x.y >> 16);
-        r[4] = (uint16_t)x.z; r[5] = (uint16_t)(x.z >> 16);
-        r[6] = (uint16_t)x.w; r[7] = (uint16_t)(x.w >> 16);
-    }
+// ---- state-row field access (row words: levels in halfwords, then values)
+__device__ __forceinline__ uint16_t w_lvl(const uint32_t *w, int k) {
+    return (uint16_t)(w[k >> 1] >> ((k & 1) * 16));
 }
-
 template <int S>
-__device__ __forceinline__ void store_row(uint16_t *base, uint32_t v, const uint16_t (&r)[S]) {
-    uint16_t *p = base + (size_t)v * S;
-    if constexpr (S == 1) {
-        p[0] = r[0];
-    } else if constexpr (S == 2) {
-        *reinterpret_cast<uint32_t *>(p) = (uint32_t)r[0] | ((uint32_t)r[1] << 16);
-    } else if constexpr (S == 4) {
-        *reinterpret_cast<uint2 *>(p) = make_uint2((uint32_t)r[0] | ((uint32_t)r[1] << 16),
-                                                  (uint32_t)r[2] | ((uint32_t)r[3] << 16));
-    } else {
-        *reinterpret_cast<uint4 *>(p) = make_uint4((uint32_t)r[0] | ((uint32_t)r[1] << 16),
-                                                  (uint32_t)r[2] | ((uint32_t)r[3] << 16),
-                                                  (uint32_t)r[4] | ((uint32_t)r[5] << 16),
-                                                  (uint32_t)r[6] | ((uint32_t)r[7] << 16));
-    }
+__device__ __forceinline__ unsigned long long w_val(const uint32_t *w, int k) {
+    constexpr int b = RowGeom<S>::kValWord;
+    return (unsigned long long)w[b + 2 * k] | ((unsigned long long)w[b + 2 * k + 1] << 32);
 }
-
-// Gathers the S 64-bit values of vertex v from one value array (one 128- or
-// 256-bit load per 32 bytes of row).
 template <int S>
-__device__ __forceinline__ void load_vals(const unsigned long long *arr, uint32_t v, unsigned long long (&x)[S]) {
-    const unsigned long long *p = arr + (size_t)v * S;
-    if constexpr (S == 1) {
-        x[0] = p[0];
-    } else if constexpr (S == 2) {
-        const ulonglong2 t = *reinterpret_cast<const ulonglong2 *>(p);
-        x[0] = t.x; x[1] = t.y;
-    } else {
+__device__ __forceinline__ unsigned char *row_of(const BatchArgs &a, uint32_t v) {
+    return a.rows + (size_t)v * RowGeom<S>::kBytes;
+}
+__device__ __forceinline__ uint16_t *lvl_at(unsigned char *row, int k) {
+    return reinterpret_cast<uint16_t *>(row) + k;
+}
+template <int S>
+__device__ __forceinline__ unsigned long long *val_at(unsigned char *row, int k) {
+    return reinterpret_cast<unsigned long long *>(row + RowGeom<S>::kLvlBytes) + k;
+}
+// Whole-row global load into words.
+template <int S>
+__device__ __forceinline__ void load_row_words(const unsigned char *row, uint32_t (&w)[RowGeom<S>::kWords]) {
+    const uint4 *p = reinterpret_cast<const uint4 *>(row);
 #pragma unroll
-        for (int h = 0; h < S; h += 4)
-            asm volatile("ld.global.v4.u64 {%0,%1,%2,%3}, [%4];"
-                         : "=l"(x[h]), "=l"(x[h + 1]), "=l"(x[h + 2]), "=l"(x[h + 3])
-                         : "l"(p + h));
+    for (int h = 0; h < RowGeom<S>::kVec; ++h) {
+        const uint4 t = p[h];
+        w[4 * h] = t.x; w[4 * h + 1] = t.y; w[4 * h + 2] = t.z; w[4 * h + 3] = t.w;
     }
 }
 
@@ -180,6 +164,11 @@ struct WarpSmem {
     uint32_t napp, nuapp;
     unsigned long long acc[kTileVerts][S];
     unsigned long long own[kTileVerts][S];
+    uint4 stage[kStageBytes / 16];  // rows gathered by cp.async, lane-sliced
+    // the tile's adjacency entries (aligned-down start, <= 256 + 3 entries)
+    alignas(16) uint32_t adjs[kTileEdges + 16];
+    // per-warp discovery totals of the sweep (LaneCounts layout)
+    unsigned long long cnt[2 + 3 * S];
 };
 
 template <int S>
@@ -203,9 +192,7 @@ struct SweepCtx {
     uint32_t key_next;   // tile mark of (batch, level d+1)
     uint32_t lb_next;    // list start of level d+1
     uint32_t next_lvl;   // d + 1 (index into lcnt)
-    const unsigned long long *src;  // value array read by the sweep's edges
-    unsigned long long *own;        // value array of level d (own sigma / X)
-    unsigned long long *dst;        // value array of level d+1 (push / pull)
+    uint32_t split;      // warps per tile (push sweeps over short lists)
 };
 
 __device__ __forceinline__ uint32_t tile_key(uint32_t b, uint32_t level) {
@@ -325,13 +312,60 @@ __device__ __forceinline__ uint32_t claim_tile(const BatchArgs &a, uint32_t w, u
     return tf;
 }
 
+// Discovery counters of one lane over one tile: (vertex, slot) pairs
+// discovered, their degrees, and per slot the count, sum of (1 + reach) and
+// sum of (deg + 2 reach).  32-bit: a lane discovers at most 8 * S pairs per tile.
 template <int S>
-__device__ __forceinline__ void flush_run(const BatchArgs &a, WarpSmem<S> &ws, int mode, uint32_t j,
+struct LaneCounts {
+    uint32_t disc = 0, pf = 0;
+    uint32_t vis[S] = {}, w[S] = {}, mc[S] = {};
+    __device__ __forceinline__ void add(int k, uint2 info) {
+        ++disc;
+        pf += info.x;
+        ++vis[k];
+        w[k] += 1u + info.y;
+        mc[k] += info.x + 2u * info.y;
+    }
+};
+
+// Warp sum of 32-bit values without overflow (16-bit halves reduced apart).
+__device__ __forceinline__ unsigned long long warp_sum32(uint32_t x) {
+    return (unsigned long long)__reduce_add_sync(0xffffffffu, x & 0xFFFFu) +
+           ((unsigned long long)__reduce_add_sync(0xffffffffu, x >> 16) << 16);
+}
+
+// Adds the warp's tile counters to its per-warp totals (all lanes call it).
+template <int S>
+__device__ __forceinline__ void flush_counts(WarpSmem<S> &ws, const LaneCounts<S> &c) {
+    if (!__any_sync(0xffffffffu, c.disc != 0)) return;
+    const unsigned long long disc = warp_sum32(c.disc), pf = warp_sum32(c.pf);
+    unsigned long long vis[S], w[S], mc[S];
+#pragma unroll
+    for (int k = 0; k < S; ++k) {
+        vis[k] = warp_sum32(c.vis[k]);
+        w[k] = warp_sum32(c.w[k]);
+        mc[k] = warp_sum32(c.mc[k]);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        ws.cnt[0] += disc;
+        ws.cnt[1] += pf;
+#pragma unroll
+        for (int k = 0; k < S; ++k) {
+            ws.cnt[2 + k] += vis[k];
+            ws.cnt[2 + S + k] += w[k];
+            ws.cnt[2 + 2 * S + k] += mc[k];
+        }
+    }
+    __syncwarp();
+}
+
+template <int S, int MODE>
+__device__ __forceinline__ void flush_run(const BatchArgs &a, WarpSmem<S> &ws, uint32_t j,
                                           unsigned long long (&run)[S]) {
 #pragma unroll
     for (int k = 0; k < S; ++k) {
         if (!run[k]) continue;
-        if (mode == kFwdPull) {
+        if (MODE == kFwdPull) {
             const unsigned long long old = atomicAdd(&ws.acc[j][k], run[k]);
             if (old + run[k] < run[k]) a.ctrl->overflow = 1;
         } else {
@@ -341,48 +375,61 @@ __device__ __forceinline__ void flush_run(const BatchArgs &a, WarpSmem<S> &ws, i
     }
 }
 
-// One tile, processed by one warp.
+// One tile (or one part of a split tile), processed by one warp.
 template <int S, int MODE>
-__device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint32_t ti, const SweepCtx &x) {
+__device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint32_t ti, const Tile &T,
+                          uint32_t part, const SweepCtx &x) {
+    constexpr int R = RowGeom<S>::kBytes;
+    constexpr int NW = RowGeom<S>::kWords;
     const unsigned lane = threadIdx.x & 31;
-    constexpr int mode = MODE;
     const uint32_t d = x.d;
     const uint16_t dl = (uint16_t)d;
-    const Tile T = a.tiles[ti];
     const bool hub = T.hub >= 0;
     const uint32_t nv = T.v1 - T.v0;
     uint32_t deg_act = 0, m = 0;
     uint2 vi = make_uint2(0, 0);
-    // ---- phase 1: activity of the tile's vertices
+    const unsigned long long pol = evict_first_policy();
+    // ---- phase 1 (one round trip): the tile's adjacency range [e0, e1) is
+    // copied to shared memory in 16-byte chunks from the aligned-down start,
+    // while each lane loads its vertex's row, degree/reach and row start
+    const uint32_t ab = T.e0 & ~3u;
+    {
+        const uint32_t nch16 = (T.e1 - ab + 3) >> 2;  // <= 65: a tile spans <= 256 entries
+        for (uint32_t c = lane; c < nch16; c += 32) cp_async16_stream(ws.adjs + 4 * c, a.adj + ab + 4 * c, pol);
+    }
+    uint32_t w[NW];
+    uint32_t ob = 0;
     if (lane < nv) {
         const uint32_t v = T.v0 + lane;
-        uint16_t l[S];
-        load_row<S>(a.lvl, v, l);
+        load_row_words<S>(row_of<S>(a, v), w);
+        vi = a.vinfo[v];
+        ob = a.offs[v];
+    }
+    cp_wait_all();
+    __syncwarp();
+    if (lane < nv) {
 #pragma unroll
         for (int k = 0; k < S; ++k) {
-            if (mode == kFwdPull) m |= (uint32_t)(l[k] == kUnvisited) << k;
-            else m |= (uint32_t)(l[k] == dl) << k;
+            const uint16_t L = w_lvl(w, k);
+            if (MODE == kFwdPull) m |= (uint32_t)(L == kUnvisited) << k;
+            else m |= (uint32_t)(L == dl) << k;
         }
+        if (MODE == kFwdPull && vi.x == 0) m = 0;  // no edge: cannot be reached
         if (m) {
-            vi = a.vinfo[v];
-            if (mode == kFwdPull && vi.x == 0) m = 0;  // no edge: cannot be reached
-        }
-        if (m) {
-            const uint32_t ob = a.offs[v];
             const uint32_t eb = hub ? T.e0 : ob;
             uint32_t ee = ob + vi.x;
             if (hub && T.e1 < ee) ee = T.e1;
             if (ee < eb) ee = eb;
             deg_act = ee - eb;
-            if (mode == kBwd && d == x.D) deg_act = 0;
+            if (MODE == kBwd && d == x.D) deg_act = 0;
             ws.eb[lane] = eb;
+            if (MODE != kFwdPush) {
 #pragma unroll
-            for (int k = 0; k < S; ++k) ws.acc[lane][k] = 0ull;
-            if (mode != kFwdPull) {
-                unsigned long long o[S];
-                load_vals<S>(x.own, v, o);
+                for (int k = 0; k < S; ++k) ws.acc[lane][k] = 0ull;
+            }
+            if (MODE != kFwdPull) {
 #pragma unroll
-                for (int k = 0; k < S; ++k) ws.own[lane][k] = ((m >> k) & 1u) ? o[k] : 0ull;
+                for (int k = 0; k < S; ++k) ws.own[lane][k] = ((m >> k) & 1u) ? w_val<S>(w, k) : 0ull;
             }
         }
         ws.mask[lane] = m;
@@ -399,10 +446,16 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
     if (lane == 0) ws.pre[nv] = total;
     __syncwarp();
 
-    // ---- phase 2: edges, a contiguous run of <= kItems per lane
-    if (total) {
-        const uint32_t i0 = lane * kItems;
-        const uint32_t i1 = min(total, i0 + kItems);
+    // ---- phase 2: this part's edges, a contiguous run of <= kItems per lane
+    uint32_t w0 = 0, w1 = total;
+    if (MODE == kFwdPush && x.split > 1) {
+        w0 = (uint32_t)(((unsigned long long)total * part) / x.split);
+        w1 = (uint32_t)(((unsigned long long)total * (part + 1)) / x.split);
+    }
+    if (w1 > w0) {
+        const uint32_t per = (w1 - w0 + 31) / 32;  // <= kItems: a tile holds <= 256 edges
+        const uint32_t i0 = w0 + lane * per;
+        const uint32_t i1 = min(w1, i0 + per);
         uint32_t j = 0;
         if (i0 < i1) {
             uint32_t lo = 0, hi = nv;
@@ -412,103 +465,125 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
             }
             j = lo;
         }
-        // edges per lane in flight, bounded by the registers their rows need
-        // (S 16-bit levels for push, S 64-bit values for pull / backward)
-        constexpr int QB = (MODE == kFwdPush) ? ((S >= 8) ? 2 : kSub) : ((S >= 8) ? 1 : (S >= 4) ? 2 : kSub);
-        const unsigned long long pol = evict_first_policy();
-        unsigned long long run[S];
+        uint32_t jj[kItems], uu[kItems];
 #pragma unroll
-        for (int k = 0; k < S; ++k) run[k] = 0ull;
-        uint32_t runj = j;
-#pragma unroll
-        for (int sub = 0; sub < kItems / QB; ++sub) {
-            uint32_t jj[QB], uu[QB];
-#pragma unroll
-            for (int q = 0; q < QB; ++q) {
-                const uint32_t i = i0 + sub * QB + q;
-                if (i < i1) {
-                    while (i >= ws.pre[j + 1]) ++j;
-                    jj[q] = j;
-                    uu[q] = ld_adj(a.adj + ws.eb[j] + (i - ws.pre[j]), pol);
-                }
+        for (int q = 0; q < kItems; ++q) {
+            const uint32_t i = i0 + q;
+            if (i < i1) {
+                while (i >= ws.pre[j + 1]) ++j;
+                jj[q] = j;
+                uu[q] = ws.adjs[ws.eb[j] - ab + (i - ws.pre[j])];
             }
-            if (mode == kFwdPush) {
-                uint16_t ul[QB][S];
+        }
+        if (MODE == kFwdPush) {
+            // stage the targets' level blocks (slot q of lane l at stage[q*32 + l],
+            // bank-conflict free), then claim / add with atomics
+            constexpr int LB = RowGeom<S>::kLvlBytes;
+            LaneCounts<S> cnt;
 #pragma unroll
-                for (int q = 0; q < QB; ++q)
-                    if (i0 + sub * QB + q < i1) load_row<S>(a.lvl, uu[q], ul[q]);
+            for (int q = 0; q < kItems; ++q) {
+                if (i0 + q >= i1) continue;
+                if (LB == 8) cp_async8(ws.stage + q * 32 + lane, row_of<S>(a, uu[q]));
+                else cp_async16(ws.stage + q * 32 + lane, row_of<S>(a, uu[q]));
+            }
+            cp_wait_all();
 #pragma unroll
-                for (int q = 0; q < QB; ++q) {
-                    uint32_t app = kNoTile;
-                    if (i0 + sub * QB + q < i1) {
-                        const uint32_t jm = ws.mask[jj[q]];
-                        const uint32_t w = uu[q];
-                        bool claimed_any = false;
-#pragma unroll
-                        for (int k = 0; k < S; ++k) {
-                            if (!((jm >> k) & 1u)) continue;
-                            const uint16_t L = ul[q][k];
-                            bool take = (L == (uint16_t)(d + 1));
-                            if (L == kUnvisited) {
-                                const uint16_t old =
-                                    atomicCAS(reinterpret_cast<unsigned short *>(a.lvl) + (size_t)w * S + k,
-                                              (unsigned short)kUnvisited, (unsigned short)(d + 1));
-                                if (old == kUnvisited) {
-                                    const uint2 wi = a.vinfo[w];
-                                    atomicAdd(&sm.c_disc, 1ull);
-                                    atomicAdd(&sm.c_pf, (unsigned long long)wi.x);
-                                    atomicAdd(&sm.c_vis[k], 1ull);
-                                    atomicAdd(&sm.c_w[k], 1ull + wi.y);
-                                    atomicAdd(&sm.c_mc[k], (unsigned long long)wi.x + 2ull * wi.y);
-                                    take = true;
-                                    claimed_any = true;
-                                } else {
-                                    take = (old == (uint16_t)(d + 1));
-                                }
-                            }
-                            if (take) {
-                                const unsigned long long s = ws.own[jj[q]][k];
-                                const unsigned long long old = atomicAdd(x.dst + (size_t)w * S + k, s);
-                                if (old + s < s) a.ctrl->overflow = 1;
-                            }
-                        }
-                        if (claimed_any) app = claim_tile(a, w, x.key_next);
-                    }
-                    append_level<S>(a, ws, app, x);
-                }
-            } else {
-                unsigned long long xv[QB][S];
-#pragma unroll
-                for (int q = 0; q < QB; ++q)
-                    if (i0 + sub * QB + q < i1) load_vals<S>(x.src, uu[q], xv[q]);
-#pragma unroll
-                for (int q = 0; q < QB; ++q) {
-                    if (i0 + sub * QB + q >= i1) continue;
-                    if (jj[q] != runj) {
-                        flush_run<S>(a, ws, mode, runj, run);
-                        runj = jj[q];
-                    }
+            for (int q = 0; q < kItems; ++q) {
+                uint32_t app = kNoTile;
+                if (i0 + q < i1) {
                     const uint32_t jm = ws.mask[jj[q]];
+                    const uint32_t wv = uu[q];
+                    const uint4 lw4 = ws.stage[q * 32 + lane];
+                    const uint32_t lwords[4] = {lw4.x, lw4.y, lw4.z, lw4.w};
+                    unsigned char *wrow = row_of<S>(a, wv);
+                    bool claimed_any = false;
 #pragma unroll
                     for (int k = 0; k < S; ++k) {
                         if (!((jm >> k) & 1u)) continue;
-                        if (mode == kFwdPull) {
-                            const unsigned long long t = run[k] + xv[q][k];
-                            if (t < xv[q][k]) a.ctrl->overflow = 1;
+                        const uint16_t L = w_lvl(lwords, k);
+                        bool take = (L == (uint16_t)(d + 1));
+                        if (L == kUnvisited) {
+                            const uint16_t old = atomicCAS(reinterpret_cast<unsigned short *>(lvl_at(wrow, k)),
+                                                           (unsigned short)kUnvisited, (unsigned short)(d + 1));
+                            if (old == kUnvisited) {
+                                cnt.add(k, a.vinfo[wv]);
+                                take = true;
+                                claimed_any = true;
+                            } else {
+                                take = (old == (uint16_t)(d + 1));
+                            }
+                        }
+                        if (take) {
+                            const unsigned long long s = ws.own[jj[q]][k];
+                            const unsigned long long old = atomicAdd(val_at<S>(wrow, k), s);
+                            if (old + s < s) a.ctrl->overflow = 1;
+                        }
+                    }
+                    if (claimed_any) app = claim_tile(a, wv, x.key_next);
+                }
+                append_level<S>(a, ws, app, x);
+            }
+            flush_counts<S>(ws, cnt);
+        } else {
+            // stage the neighbours' whole rows, then sum the matching values
+            constexpr int E = (kStageBytes / (32 * R)) < kItems ? (kStageBytes / (32 * R)) : kItems;
+            static_assert(kItems % E == 0, "staging rounds must divide the run");
+            const uint16_t want = (MODE == kFwdPull) ? dl : (uint16_t)(d + 1);
+            // 16-byte chunk h of lane l's row q sits at stage[(q*H + h)*32 + l]:
+            // a warp's accesses hit 32 consecutive 16-byte slots (no bank conflicts)
+            constexpr int H = R / 16;
+            unsigned long long run[S];
+#pragma unroll
+            for (int k = 0; k < S; ++k) run[k] = 0ull;
+            uint32_t runj = (i0 < i1) ? jj[0] : 0u;
+#pragma unroll
+            for (int r = 0; r < kItems / E; ++r) {
+#pragma unroll
+                for (int q = 0; q < E; ++q) {
+                    const int idx = r * E + q;
+                    if (i0 + idx < i1) {
+                        const uint4 *src = reinterpret_cast<const uint4 *>(row_of<S>(a, uu[idx]));
+#pragma unroll
+                        for (int h = 0; h < H; ++h) cp_async16(ws.stage + (q * H + h) * 32 + lane, src + h);
+                    }
+                }
+                cp_wait_all();
+#pragma unroll
+                for (int q = 0; q < E; ++q) {
+                    const int idx = r * E + q;
+                    if (i0 + idx >= i1) continue;
+                    if (jj[idx] != runj) {
+                        flush_run<S, MODE>(a, ws, runj, run);
+                        runj = jj[idx];
+                    }
+                    const uint32_t jm = ws.mask[jj[idx]];
+                    uint32_t wr[RowGeom<S>::kWords];
+#pragma unroll
+                    for (int h = 0; h < H; ++h) {
+                        const uint4 t = ws.stage[(q * H + h) * 32 + lane];
+                        wr[4 * h] = t.x; wr[4 * h + 1] = t.y; wr[4 * h + 2] = t.z; wr[4 * h + 3] = t.w;
+                    }
+#pragma unroll
+                    for (int k = 0; k < S; ++k) {
+                        if (!((jm >> k) & 1u) || w_lvl(wr, k) != want) continue;
+                        const unsigned long long xv = w_val<S>(wr, k);
+                        if (MODE == kFwdPull) {
+                            const unsigned long long t = run[k] + xv;
+                            if (t < xv) a.ctrl->overflow = 1;
                             run[k] = t;
                         } else {
-                            const double t = __longlong_as_double((long long)run[k]) +
-                                             __longlong_as_double((long long)xv[q][k]);
+                            const double t =
+                                __longlong_as_double((long long)run[k]) + __longlong_as_double((long long)xv);
                             run[k] = (unsigned long long)__double_as_longlong(t);
                         }
                     }
                 }
             }
+            if (i0 < i1) flush_run<S, MODE>(a, ws, runj, run);
         }
-        if (mode != kFwdPush && i0 < i1) flush_run<S>(a, ws, mode, runj, run);
     }
     __syncwarp();
-    if (mode == kFwdPush) return;
+    if (MODE == kFwdPush) return;
 
     // ---- hub chunks meet in hub_acc; the last chunk to arrive finishes the vertex
     if (hub) {
@@ -516,7 +591,7 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
         unsigned long long *hacc = a.hub_acc + (size_t)T.hub * S;
         if (lane < (unsigned)S && ((hm >> lane) & 1u)) {
             const unsigned long long xa = ws.acc[0][lane];
-            if (mode == kFwdPull) {
+            if (MODE == kFwdPull) {
                 const unsigned long long old = atomicAdd(hacc + lane, xa);
                 if (old + xa < xa) a.ctrl->overflow = 1;
             } else {
@@ -537,9 +612,11 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
 
     // ---- phase 3: finish the tile's vertices
     uint32_t nd = 0, left = 0;
+    LaneCounts<S> cnt;
     if (lane < nv && m) {
         const uint32_t v = T.v0 + lane;
-        if (mode == kFwdPull) {
+        unsigned char *vrow = row_of<S>(a, v);
+        if (MODE == kFwdPull) {
 #pragma unroll
             for (int k = 0; k < S; ++k) {
                 if (!((m >> k) & 1u)) continue;
@@ -548,16 +625,10 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
                     ++left;
                     continue;
                 }
-                a.lvl[(size_t)v * S + k] = (uint16_t)(d + 1);
-                x.dst[(size_t)v * S + k] = s;
+                *lvl_at(vrow, k) = (uint16_t)(d + 1);
+                *val_at<S>(vrow, k) = s;
                 ++nd;
-                atomicAdd(&sm.c_vis[k], 1ull);
-                atomicAdd(&sm.c_w[k], 1ull + vi.y);
-                atomicAdd(&sm.c_mc[k], (unsigned long long)vi.x + 2ull * vi.y);
-            }
-            if (nd) {
-                atomicAdd(&sm.c_disc, (unsigned long long)nd);
-                atomicAdd(&sm.c_pf, (unsigned long long)nd * vi.x);
+                cnt.add(k, vi);
             }
         } else {
             double add = 0.0;
@@ -569,14 +640,15 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
                 const double acc = __longlong_as_double((long long)ws.acc[lane][k]);
                 const double delta = reach + sig * acc;
                 const double xo = (1.0 + delta) / sig;
-                x.own[(size_t)v * S + k] = (unsigned long long)__double_as_longlong(xo);
+                *val_at<S>(vrow, k) = (unsigned long long)__double_as_longlong(xo);
                 if (d > 0) add += sm.mult[k] * delta;
                 if (a.dbg_delta) a.dbg_delta[v] = delta;
             }
             if (d > 0) a.bc[v] += add;
         }
     }
-    if (mode == kFwdPull) {
+    if (MODE == kFwdPull) {
+        flush_counts<S>(ws, cnt);
         // a pull sweep visits every listed tile once, so no mark is needed; a
         // hub is listed by its finishing chunk (first chunk | kHubFlag expands it)
         const uint32_t me = hub ? a.tile_of[T.v0] : ti;
@@ -588,7 +660,8 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
 }
 
 // Runs one sweep: every warp of the grid walks its share of the work items,
-// item i being list[i % ring] (or tile i when list is null).
+// item i being list[(start + i) % ring] (or tile i when list is null); with
+// x.split > 1 each item is cut into x.split parts handed to different warps.
 template <int S>
 __device__ void run_sweep(const BatchArgs &a, Smem<S> &sm, const SweepCtx &x, const uint32_t *list,
                           unsigned long long start, uint32_t nwork, unsigned long long ring) {
@@ -596,13 +669,35 @@ __device__ void run_sweep(const BatchArgs &a, Smem<S> &sm, const SweepCtx &x, co
     WarpSmem<S> &ws = sm.w[wid];
     const uint32_t gw = blockIdx.x * kWarps + wid;
     const uint32_t nw = gridDim.x * kWarps;
-    if ((threadIdx.x & 31) == 0) { ws.napp = 0; ws.nuapp = 0; }
+    if ((threadIdx.x & 31) == 0) {
+        ws.napp = 0;
+        ws.nuapp = 0;
+#pragma unroll
+        for (int q = 0; q < 2 + 3 * S; ++q) ws.cnt[q] = 0ull;
+    }
     __syncwarp();
-    for (uint32_t i = gw; i < nwork; i += nw) {
-        const uint32_t ti = list ? list[(start + i) % ring] : i;
-        if (x.mode == kFwdPush) warp_tile<S, kFwdPush>(a, sm, ws, ti, x);
-        else if (x.mode == kFwdPull) warp_tile<S, kFwdPull>(a, sm, ws, ti, x);
-        else warp_tile<S, kBwd>(a, sm, ws, ti, x);
+    const unsigned long long nitems = (unsigned long long)nwork * x.split;
+    auto item_tile = [&](unsigned long long it) -> uint32_t {
+        const uint32_t i = (uint32_t)(it / x.split);
+        return list ? list[(start + i) % ring] : i;
+    };
+    // software prefetch: the descriptor of the next item and the list entry of
+    // the one after are loaded one iteration ahead of their use
+    unsigned long long it = gw;
+    uint32_t ti1 = (it < nitems) ? item_tile(it) : 0u;
+    uint32_t ti2 = (it + nw < nitems) ? item_tile(it + nw) : 0u;
+    Tile T1{};
+    if (it < nitems) T1 = a.tiles[ti1];
+    for (; it < nitems; it += nw) {
+        const uint32_t part = (uint32_t)(it % x.split);
+        const uint32_t ti = ti1;
+        const Tile T = T1;
+        if (it + nw < nitems) T1 = a.tiles[ti2];
+        ti1 = ti2;
+        if (it + 2ull * nw < nitems) ti2 = item_tile(it + 2ull * nw);
+        if (x.mode == kFwdPush) warp_tile<S, kFwdPush>(a, sm, ws, ti, T, part, x);
+        else if (x.mode == kFwdPull) warp_tile<S, kFwdPull>(a, sm, ws, ti, T, 0, x);
+        else warp_tile<S, kBwd>(a, sm, ws, ti, T, 0, x);
         __syncwarp();
     }
     if (x.mode != kBwd) {
@@ -610,23 +705,30 @@ __device__ void run_sweep(const BatchArgs &a, Smem<S> &sm, const SweepCtx &x, co
         if (cnt) flush_level<S>(a, ws, cnt, x);
         const uint32_t ucnt = ws.nuapp;
         if (ucnt) flush_unvisited<S>(a, ws, ucnt);
+        // per-warp discovery totals into the CTA's counters
+        if ((threadIdx.x & 31) == 0 && ws.cnt[0]) {
+            atomicAdd(&sm.c_disc, ws.cnt[0]);
+            atomicAdd(&sm.c_pf, ws.cnt[1]);
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+                atomicAdd(&sm.c_vis[k], ws.cnt[2 + k]);
+                atomicAdd(&sm.c_w[k], ws.cnt[2 + S + k]);
+                atomicAdd(&sm.c_mc[k], ws.cnt[2 + 2 * S + k]);
+            }
+        }
     }
 }
 
-// CTAs per SM the register allocation is sized for (2: 64 registers/thread).
-#ifndef BCG_MIN_BLOCKS
-#define BCG_MIN_BLOCKS 2
-#endif
-
 template <int S>
-__global__ void __launch_bounds__(kThreads, BCG_MIN_BLOCKS) bc_sweep_kernel(BatchArgs a) {
+__global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem<S> &sm = *reinterpret_cast<Smem<S> *>(smem_raw);
+    constexpr int R = RowGeom<S>::kBytes;
     Ctrl *c = a.ctrl;
     const unsigned int nblk = gridDim.x;
     const unsigned long long wait_ns = c->wait_ns ? c->wait_ns : kDefaultWaitNs;
-    const size_t plane = (size_t)a.n * S;  // distance between the three value arrays
     const unsigned long long ring = 2ull * a.ntiles;
+    const uint32_t total_warps = gridDim.x * kWarps;
 
     for (uint32_t b = 0; b < a.nbatch; ++b) {
         if (threadIdx.x < S) {
@@ -670,19 +772,24 @@ __global__ void __launch_bounds__(kThreads, BCG_MIN_BLOCKS) bc_sweep_kernel(Batc
             }
             a.lcnt[0] = n0;
         }
-        // reset every row; roots at level 0 with sigma 1 (array 0)
+        // reset every row; roots at level 0 with sigma 1
         for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < a.n;
              v += (size_t)gridDim.x * blockDim.x) {
-            uint16_t l[S];
+            constexpr int VW = RowGeom<S>::kValWord;
+            uint32_t w[R / 4];
+#pragma unroll
+            for (int q = 0; q < VW; ++q) w[q] = 0xFFFFFFFFu;  // all levels unvisited
+#pragma unroll
+            for (int q = VW; q < R / 4; ++q) w[q] = 0u;
 #pragma unroll
             for (int k = 0; k < S; ++k) {
-                const bool r = (sm.roots[k] == (uint32_t)v);
-                l[k] = r ? (uint16_t)0 : kUnvisited;
-                a.val[v * S + k] = r ? 1ull : 0ull;
-                a.val[plane + v * S + k] = 0ull;
-                a.val[2 * plane + v * S + k] = 0ull;
+                if (sm.roots[k] != (uint32_t)v) continue;
+                w[k >> 1] &= ~(0xFFFFu << ((k & 1) * 16));  // level 0
+                w[VW + 2 * k] = 1u;                         // sigma 1
             }
-            store_row<S>(a.lvl, (uint32_t)v, l);
+            uint4 *p = reinterpret_cast<uint4 *>(a.rows + v * R);
+#pragma unroll
+            for (int h = 0; h < R / 16; ++h) p[h] = make_uint4(w[4 * h], w[4 * h + 1], w[4 * h + 2], w[4 * h + 3]);
         }
         if (!grid_sync(c, nblk, wait_ns)) return;
         trace(a, b, 0, 0, 0, 0);
@@ -692,6 +799,10 @@ __global__ void __launch_bounds__(kThreads, BCG_MIN_BLOCKS) bc_sweep_kernel(Batc
         bool uall = true;              // no pull sweep yet: every tile may hold unvisited vertices
         unsigned long long ustart = 0; // ring position / length of the unvisited-tile list
         uint32_t ulen = 0;
+        // ring write position; only pull sweeps move it, so it is read only
+        // right after a barrier (here: after the init barrier), never at the
+        // start of a sweep where a faster CTA may already have appended
+        unsigned long long ucur = vload64(&c->uctr);
         for (;;) {
             SweepCtx x;
             x.mode = (!a.directed && (double)pf_cur >= (double)a.push_pull_ratio * (double)pu_cur) ? kFwdPull
@@ -703,10 +814,7 @@ __global__ void __launch_bounds__(kThreads, BCG_MIN_BLOCKS) bc_sweep_kernel(Batc
             x.lb_next = lb + lc;
             x.next_lvl = d + 1;
             x.key_next = tile_key(b, d + 1);
-            x.own = a.val + (size_t)(d % 3) * plane;
-            x.src = x.own;
-            x.dst = a.val + (size_t)((d + 1) % 3) * plane;
-            const unsigned long long ubefore = vload64(&c->uctr);
+            x.split = (x.mode == kFwdPush && lc * 2 < total_warps) ? kPushSplit : 1;
             if (threadIdx.x == 0) {
                 sm.c_disc = 0; sm.c_pf = 0;
 #pragma unroll
@@ -748,8 +856,9 @@ __global__ void __launch_bounds__(kThreads, BCG_MIN_BLOCKS) bc_sweep_kernel(Batc
             trace(a, b, x.mode == kFwdPull ? 2u : 1u, d, walked, disc);
             if (x.mode == kFwdPull) {
                 const unsigned long long uafter = vload64(&c->uctr);
-                ustart = ubefore;
-                ulen = (uint32_t)(uafter - ubefore);
+                ustart = ucur;
+                ulen = (uint32_t)(uafter - ucur);
+                ucur = uafter;
                 uall = false;
             }
             if (disc == 0) break;
@@ -764,10 +873,11 @@ __global__ void __launch_bounds__(kThreads, BCG_MIN_BLOCKS) bc_sweep_kernel(Batc
         const uint32_t D = d;
 
         if (a.dbg_sigma) {
+            // single-slot debug run: copy sigma out before the backward pass
             for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < a.n;
                  v += (size_t)gridDim.x * blockDim.x) {
-                const uint16_t L = a.lvl[v * S];
-                a.dbg_sigma[v] = (L == kUnvisited) ? 0ull : a.val[(size_t)(L % 3) * plane + v * S];
+                unsigned char *row = a.rows + v * R;
+                a.dbg_sigma[v] = (*lvl_at(row, 0) == kUnvisited) ? 0ull : *val_at<S>(row, 0);
             }
             if (!grid_sync(c, nblk, wait_ns)) return;
         }
@@ -782,9 +892,7 @@ __global__ void __launch_bounds__(kThreads, BCG_MIN_BLOCKS) bc_sweep_kernel(Batc
             x.key_next = 0;
             x.lb_next = 0;
             x.next_lvl = 0;
-            x.own = a.val + (size_t)(dd % 3) * plane;
-            x.src = a.val + (size_t)((dd + 1) % 3) * plane;
-            x.dst = nullptr;
+            x.split = 1;
             const uint32_t lb = vload32(a.lbase + dd);
             const uint32_t lc = vload32(a.lcnt + dd);
             run_sweep<S>(a, sm, x, a.lists + lb, 0, lc, 0xFFFFFFFFull);
@@ -841,10 +949,9 @@ static int launch_impl(const BatchArgs &a, cudaStream_t st, int *grid_out) {
 int launch_sweep(int S, const BatchArgs &a, cudaStream_t st, int *grid_out) {
     switch (S) {
         case 1: return launch_impl<1>(a, st, grid_out);
-        case 2: return launch_impl<2>(a, st, grid_out);
-        case 4: return launch_impl<4>(a, st, grid_out);
-        case 8: return launch_impl<8>(a, st, grid_out);
-        default: return set_error(BCG_ERR_ARG, "batch width %d not in {1,2,4,8}", S);
+        case 3: return launch_impl<3>(a, st, grid_out);
+        case 6: return launch_impl<6>(a, st, grid_out);
+        default: return set_error(BCG_ERR_ARG, "batch width %d not in {1,3,6}", S);
     }
 }
 

@@ -198,7 +198,7 @@ int bcg_graph_set_reach(bcg_graph *g, const uint32_t *reach);
 int bcg_run_weighted(bcg_graph *g, const uint32_t *roots, const double *mult,
                      const uint32_t *pend, uint64_t nroots, bcg_stats *stats);
 
-/* Forces the sources-per-batch width (1, 2, 4 or 8; 0 = automatic). */
+/* Forces the sources-per-batch width (1, 3 or 6; 0 = automatic). */
 int bcg_set_batch_width(bcg_graph *g, uint32_t width);
 
 /* Message for the last error of the calling thread ("" if none). */

@@ -100,7 +100,7 @@ def test_bc_matches_oracle(graphs, gname, flags):
         assert st.max_depth == ost["max_depth"] or flags
 
 
-@pytest.mark.parametrize("width", [1, 2, 4, 8])
+@pytest.mark.parametrize("width", [1, 3, 6])
 def test_batch_widths_agree(graphs, width):
     offs, adj = graphs["rmat11_pend"]
     src = bcg.sample_sources(len(offs) - 1, 37, 5)
@@ -142,7 +142,7 @@ def test_hub_chunks_all_modes():
     offs, adj = bcg.from_pairs(pairs, n)
     src = [0, 1, 4500, k + 2, 17]
     ref, _ = oracle.bc(offs, adj, src)
-    for ratio_width in (1, 4, 8):
+    for ratio_width in (1, 3, 6):
         with bcg.Graph(offs, adj) as G:
             G.set_batch_width(ratio_width)
             G.run(src)
