@@ -5,12 +5,19 @@
 
 namespace bcg {
 
-constexpr int kThreads = 512;            // threads per CTA of the sweep kernel
+// Sweep kernel geometry (one CTA per SM; the build may override both).
+#ifndef BCG_THREADS
+#define BCG_THREADS 512
+#endif
+#ifndef BCG_STAGE_BYTES
+#define BCG_STAGE_BYTES 8192
+#endif
+constexpr int kThreads = BCG_THREADS;    // threads per CTA of the sweep kernel
 constexpr int kWarps = kThreads / 32;    // independent tile workers per CTA
 constexpr int kTileVerts = 32;           // max vertices per tile (one per lane)
 constexpr int kTileEdges = 256;          // max adjacency entries per tile
 constexpr int kItems = kTileEdges / 32;  // edges per lane per tile
-constexpr int kStageBytes = 8192;        // per-warp shared staging of gathered rows
+constexpr int kStageBytes = BCG_STAGE_BYTES;  // per-warp shared staging of gathered rows
 constexpr int kPushSplit = 8;            // sparse push sweeps: warps per tile
 constexpr uint16_t kUnvisited = 0xFFFFu;
 constexpr uint32_t kMaxLevel = 0xFFFDu;  // deepest level a 16-bit level can hold

@@ -171,6 +171,9 @@ struct WarpSmem {
     unsigned long long cnt[2 + 3 * S];
 };
 
+// push sweeps stage one 16-byte level block per edge of the lane's run
+static_assert(kStageBytes >= kItems * 32 * 16, "stage must hold a push tile's level blocks");
+
 template <int S>
 struct Smem {
     WarpSmem<S> w[kWarps];
@@ -180,6 +183,7 @@ struct Smem {
     // batch constants
     uint32_t roots[S];
     double mult[S];
+    uint32_t next;  // work items drawn by this CTA's warps in the current sweep
 };
 
 template <int S>
@@ -659,16 +663,18 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
     }
 }
 
-// Runs one sweep: every warp of the grid walks its share of the work items,
-// item i being list[(start + i) % ring] (or tile i when list is null); with
-// x.split > 1 each item is cut into x.split parts handed to different warps.
+// Runs one sweep: the grid walks the work items, item i being
+// list[(start + i) % ring] (or tile i when list is null); with x.split > 1
+// each item is cut into x.split parts handed to different warps.  CTA b owns
+// items b, b + G, b + 2G, ... (G CTAs: every CTA gets a slice of every region
+// of the list), and its warps take them one at a time from a shared counter
+// (sm.next, zeroed before the sweep), so a warp that drew cheap tiles keeps
+// working instead of waiting at the sweep's barrier.
 template <int S>
 __device__ void run_sweep(const BatchArgs &a, Smem<S> &sm, const SweepCtx &x, const uint32_t *list,
                           unsigned long long start, uint32_t nwork, unsigned long long ring) {
     const unsigned wid = threadIdx.x >> 5;
     WarpSmem<S> &ws = sm.w[wid];
-    const uint32_t gw = blockIdx.x * kWarps + wid;
-    const uint32_t nw = gridDim.x * kWarps;
     if ((threadIdx.x & 31) == 0) {
         ws.napp = 0;
         ws.nuapp = 0;
@@ -681,24 +687,35 @@ __device__ void run_sweep(const BatchArgs &a, Smem<S> &sm, const SweepCtx &x, co
         const uint32_t i = (uint32_t)(it / x.split);
         return list ? list[(start + i) % ring] : i;
     };
-    // software prefetch: the descriptor of the next item and the list entry of
-    // the one after are loaded one iteration ahead of their use
-    unsigned long long it = gw;
+    const unsigned long long G = gridDim.x;
+    auto grab = [&]() -> unsigned long long {
+        unsigned long long c = 0;
+        if ((threadIdx.x & 31) == 0) c = atomicAdd(&sm.next, 1u);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        return blockIdx.x + c * G;
+    };
+    // software prefetch: each warp holds two drawn items; the descriptor of the
+    // next one and the list entry of the one after are loaded an iteration early
+    unsigned long long it = grab();
+    unsigned long long it2 = (it < nitems) ? grab() : nitems;
     uint32_t ti1 = (it < nitems) ? item_tile(it) : 0u;
-    uint32_t ti2 = (it + nw < nitems) ? item_tile(it + nw) : 0u;
+    uint32_t ti2 = (it2 < nitems) ? item_tile(it2) : 0u;
     Tile T1{};
     if (it < nitems) T1 = a.tiles[ti1];
-    for (; it < nitems; it += nw) {
+    while (it < nitems) {
         const uint32_t part = (uint32_t)(it % x.split);
         const uint32_t ti = ti1;
         const Tile T = T1;
-        if (it + nw < nitems) T1 = a.tiles[ti2];
+        const unsigned long long it_next = it2;
+        if (it2 < nitems) T1 = a.tiles[ti2];
         ti1 = ti2;
-        if (it + 2ull * nw < nitems) ti2 = item_tile(it + 2ull * nw);
+        it2 = (it2 < nitems) ? grab() : nitems;
+        if (it2 < nitems) ti2 = item_tile(it2);
         if (x.mode == kFwdPush) warp_tile<S, kFwdPush>(a, sm, ws, ti, T, part, x);
         else if (x.mode == kFwdPull) warp_tile<S, kFwdPull>(a, sm, ws, ti, T, 0, x);
         else warp_tile<S, kBwd>(a, sm, ws, ti, T, 0, x);
         __syncwarp();
+        it = it_next;
     }
     if (x.mode != kBwd) {
         const uint32_t cnt = ws.napp;
@@ -816,6 +833,7 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
             x.key_next = tile_key(b, d + 1);
             x.split = (x.mode == kFwdPush && lc * 2 < total_warps) ? kPushSplit : 1;
             if (threadIdx.x == 0) {
+                sm.next = 0;
                 sm.c_disc = 0; sm.c_pf = 0;
 #pragma unroll
                 for (int k = 0; k < S; ++k) { sm.c_vis[k] = 0; sm.c_w[k] = 0; sm.c_mc[k] = 0; }
@@ -895,6 +913,8 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
             x.split = 1;
             const uint32_t lb = vload32(a.lbase + dd);
             const uint32_t lc = vload32(a.lcnt + dd);
+            if (threadIdx.x == 0) sm.next = 0;
+            __syncthreads();
             run_sweep<S>(a, sm, x, a.lists + lb, 0, lc, 0xFFFFFFFFull);
             if (!grid_sync(c, nblk, wait_ns)) return;
             trace(a, b, 3u, (uint32_t)dd, lc, 0);
