@@ -20,7 +20,7 @@
 //     the aggregate rate (sum of component edges / kernel time / 2^20).
 // Extensions (letters unused by the reference): -s <file> source list (one id
 // per line), -F full-precision output ("%.17g" of bc/2), -G <spec> generator
-// spec (see bcg_csr_generate), -W <1|2|4|8> sources per batch.
+// spec (see bcg_csr_generate), -W <1|3|6> sources per batch.
 #include <getopt.h>
 #include <sys/time.h>
 
@@ -65,7 +65,7 @@ static double now_us() {
            "\t\t -s <file> list of source vertices (one id per line)\n"
            "\t\t -F write bc/2 with full precision (%%.17g)\n"
            "\t\t -G <spec> generate a graph (rmat:/er:/grid: spec)\n"
-           "\t\t -W <1|2|4|8> sources per batch\n"
+           "\t\t -W <1|3|6> sources per batch\n"
            "\n",
            pname);
 }

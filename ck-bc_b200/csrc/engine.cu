@@ -7,13 +7,14 @@
 //   per-source loop + skip        bc2d.c:1016-1050
 //   get_bc                        cuda_kernels.cu:1039-1041
 //
-// Degree-1 pruning (north_star (a)).  A vertex p of degree 1 whose neighbour a
+// Degree-1 pruning pre-pass.  A vertex p of degree 1 whose neighbour a
 // does not also have degree 1 is folded into a: p leaves the traversal graph
 // and reach[a] counts it.  For an isolated edge {p, a} (both degree 1) the
 // larger id is folded into the smaller.  The pruned graph keeps the vertex
 // ids and the CSR row starts; each surviving list is compacted to the front of
 // its row and vinfo[v].x holds its new length.  Exact BC is preserved by
-// weighting (derivation in DESIGN.md):
+// weighting (Brandes' dependency sum split by which side of the folded edge
+// each endpoint lies on):
 //   - the backward pass starts every delta at reach[v] (init_delta,
 //     cuda_kernels.cu:1089-1098), so pendants count as targets;
 //   - a source s folded into anchor a runs as a BFS from a; the root's

@@ -6,7 +6,7 @@
  * the cuda_kernels.cu implementation named beside it, so that the
  * reference's host driver bc2d.c compiles unmodified and links against this
  * library instead of cuda_kernels.cu (recipe: oracle/Makefile target
- * ref-compat; walk-through in INTEGRATION.md).  LOCINT is the reference's
+ * ref-compat).  LOCINT is the reference's
  * 32-bit vertex id (bc2d.h:14).
  *
  * Semantics kept: the same call order and per-level return values as the

@@ -180,6 +180,53 @@ int oracle_bc(uint32_t n, const uint32_t *offs, const uint32_t *adj, const uint3
     return err ? -1 : 0;
 }
 
+/* Sum over the given sources (degree 0 skipped) and every vertex t != s
+ * reachable from s of (d(s,t) - 1).  Brandes' dependencies satisfy
+ * sum_v delta_s(v) = sum_t (d(s,t) - 1) (each shortest s-t path has d - 1
+ * interior vertices and the pair's weights sum to one per interior position),
+ * so this is the exact total of bc[] over a source set: a size-independent
+ * check that needs only a BFS per source. */
+int oracle_path_length_sum(uint32_t n, const uint32_t *offs, const uint32_t *adj, const uint32_t *sources,
+                           uint64_t nsrc, int nthreads, uint64_t *total) {
+    int nt = nthreads > 0 ? nthreads : 1;
+#ifndef _OPENMP
+    nt = 1;
+#endif
+    uint64_t sum = 0;
+    int err = 0;
+#pragma omp parallel num_threads(nt) reduction(+ : sum) reduction(| : err)
+    {
+        int32_t *lvl = (int32_t *)malloc((size_t)n * sizeof(int32_t));
+        uint32_t *queue = (uint32_t *)malloc((size_t)n * sizeof(uint32_t));
+        if (!lvl || !queue) err = 1;
+#pragma omp for schedule(dynamic, 1)
+        for (int64_t i = 0; i < (int64_t)nsrc; ++i) {
+            if (err) continue;
+            uint32_t s = sources[i];
+            if (s >= n) { err = 1; continue; }
+            if (offs[s + 1] == offs[s]) continue;
+            for (uint32_t v = 0; v < n; ++v) lvl[v] = -1;
+            uint32_t head = 0, tail = 0;
+            lvl[s] = 0;
+            queue[tail++] = s;
+            while (head < tail) {
+                uint32_t c = queue[head++];
+                for (uint32_t e = offs[c]; e < offs[c + 1]; ++e) {
+                    uint32_t r = adj[e];
+                    if (lvl[r] == -1) {
+                        lvl[r] = lvl[c] + 1;
+                        queue[tail++] = r;
+                        sum += (uint64_t)lvl[r] - 1;
+                    }
+                }
+            }
+        }
+        free(lvl); free(queue);
+    }
+    if (total) *total = sum;
+    return err ? -1 : 0;
+}
+
 int oracle_max_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

@@ -17,5 +17,9 @@ int oracle_single_source(uint32_t n, const uint32_t *offs, const uint32_t *adj, 
 /* Adds every source's dependencies into bc[n] (ordered-pair sums). */
 int oracle_bc(uint32_t n, const uint32_t *offs, const uint32_t *adj, const uint32_t *sources,
               uint64_t nsrc, int nthreads, double *bc, oracle_stats *st);
+/* Sum over sources (degree 0 skipped) and reachable t != s of (d(s,t) - 1):
+ * the exact total of bc[] over that source set. */
+int oracle_path_length_sum(uint32_t n, const uint32_t *offs, const uint32_t *adj, const uint32_t *sources,
+                           uint64_t nsrc, int nthreads, uint64_t *total);
 int oracle_max_threads(void);
 #endif

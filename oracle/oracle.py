@@ -47,6 +47,9 @@ def lib():
         L.oracle_bc.argtypes = [ctypes.c_uint32, _u32p, _u32p, _u32p, ctypes.c_uint64, ctypes.c_int, _f64p,
                                 ctypes.POINTER(OracleStats)]
         L.oracle_max_threads.restype = ctypes.c_int
+        L.oracle_path_length_sum.restype = ctypes.c_int
+        L.oracle_path_length_sum.argtypes = [ctypes.c_uint32, _u32p, _u32p, _u32p, ctypes.c_uint64, ctypes.c_int,
+                                             _u64p]
         _LIB = L
     return _LIB
 
@@ -83,6 +86,20 @@ def bc(offsets, adj, sources, nthreads: int = 1):
     if rc:
         raise RuntimeError(f"oracle_bc failed ({rc})")
     return out, {f: getattr(st, f) for f, _ in st._fields_}
+
+
+def path_length_sum(offsets, adj, sources, nthreads: int = 1) -> int:
+    """Sum over sources (degree 0 skipped) and reachable t != s of d(s,t) - 1,
+    which equals the sum of bc[] over that source set (exact integer)."""
+    offsets, adj = _u32(offsets), _u32(adj)
+    s = _u32(sources)
+    n = len(offsets) - 1
+    tot = ctypes.c_uint64(0)
+    rc = lib().oracle_path_length_sum(n, offsets.ctypes.data_as(_u32p), adj.ctypes.data_as(_u32p),
+                                      s.ctypes.data_as(_u32p), len(s), nthreads, ctypes.byref(tot))
+    if rc:
+        raise RuntimeError(f"oracle_path_length_sum failed ({rc})")
+    return int(tot.value)
 
 
 def max_threads() -> int:

@@ -1,11 +1,11 @@
 """Runs the reference program (ck-bc program/bc-cuda, built from its own
-sources by `make -C oracle ref` into oracle/_ref/bc2d_ref) on the config-1
-graph and stores its result file as a fixture:
+sources by `make -C oracle ref` into oracle/_ref/bc2d_ref) on the R-MAT
+scale-12 graph and stores its result file as a fixture:
 
   tests/golden/ref_rmat12_s1_N4096.txt   reference output, "%d\\t%.2f" of bc/2
   tests/golden/rmat12_s1.txt             (not kept) edge list it was run on
 
-Config 1: R-MAT scale 12, edge factor 16, (a,b,c,d) = (0.57,0.19,0.19,0.05),
+Graph: R-MAT scale 12, edge factor 16, (a,b,c,d) = (0.57,0.19,0.19,0.05),
 seed 1, undirected, duplicates and self-loops removed; all 4096 sources
 (bc2d -p 1x1 -f <file> -n 4096 -r 0 -N 4096, no pruning).
 

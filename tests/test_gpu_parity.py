@@ -1,6 +1,6 @@
 """GPU parity: the CUDA engine (through the C ABI) against the CPU oracle.
 
-Bars (north_star): BFS depths and sigma bit-exact; delta and bc within
+Bars: BFS depths and sigma bit-exact; delta and bc within
 1e-9 relative, written here as |gpu - oracle| <= 1e-9 * max(|oracle|, 1)."""
 import numpy as np
 import pytest
@@ -27,7 +27,7 @@ def _golden_csr(g):
 
 GRAPHS = {
     "rmat10": "rmat:scale=10,ef=16,seed=11",
-    "rmat12_c1": "rmat:scale=12,ef=16,a=0.57,b=0.19,c=0.19,seed=1",
+    "rmat12_s1": "rmat:scale=12,ef=16,a=0.57,b=0.19,c=0.19,seed=1",
     "er11": "er:scale=11,ef=8,seed=4",
     "grid40": "grid:w=40,h=30,drop=0.05,seed=3",
     "rmat11_pend": "rmat:scale=11,ef=8,seed=9,pendant_frac=0.1,pendant_mean=4",
@@ -205,15 +205,15 @@ def test_one_shot_matches_handle(graphs):
     assert_bc_close(bc1, ref, "one-shot")
 
 
-def test_c1_config_full():
-    """Config 1: R-MAT scale 12, ef 16, (0.57,0.19,0.19,0.05), seed 1, all sources."""
+def test_rmat12_all_sources_full():
+    """R-MAT scale 12, ef 16, (0.57,0.19,0.19,0.05), seed 1, all sources."""
     offs, adj = bcg.generate("rmat:scale=12,ef=16,a=0.57,b=0.19,c=0.19,seed=1")
     n = len(offs) - 1
     src = np.arange(n, dtype=np.uint32)
     ref, ost = oracle.bc(offs, adj, src, nthreads=oracle.max_threads())
     with bcg.Graph(offs, adj) as G:
         st = G.run(src)
-        assert_bc_close(G.bc(), ref, "C1")
+        assert_bc_close(G.bc(), ref, "rmat12 all sources")
         assert st.teps_edges == ost["teps_edges"]
     for s in (0, 1, 100, 4095):
         if offs[s + 1] == offs[s]:
@@ -222,4 +222,4 @@ def test_c1_config_full():
             lvl, sig, dl = G.single_source(s)
         olvl, osig, odl, _ = oracle.single_source(offs, adj, s)
         assert np.array_equal(lvl, olvl) and np.array_equal(sig, osig)
-        assert_bc_close(dl, odl, f"C1 delta s={s}")
+        assert_bc_close(dl, odl, f"rmat12 delta s={s}")

@@ -169,8 +169,8 @@ def test_bad_specs():
             bcg.generate(spec)
 
 
-def test_c2_graph_shape():
-    """Config 2 graph: R-MAT s20 ef16 + pendant trees on 10% (mean size 4)."""
+def test_benchmark_graph_shape():
+    """Benchmark graph: R-MAT s20 ef16 + pendant trees on 10% (mean size 4)."""
     if os.environ.get("BCG_SKIP_BIG"):
         pytest.skip("big graph disabled")
     offs, adj = bcg.generate("rmat:scale=20,ef=16,a=0.57,b=0.19,c=0.19,seed=2,pendant_frac=0.1,pendant_mean=4")

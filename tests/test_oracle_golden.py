@@ -87,3 +87,17 @@ def test_pendant_golden_includes_tree_internal_vertices(golden, name):
     g = golden["graphs"][name]
     # vertex 5 sits inside a depth-2 pendant tree: its bc is non-zero
     assert g["bc_half"][5] > 0
+
+
+def test_path_length_sum_identity(golden):
+    """sum_v bc[v] = sum over sources s and reachable t != s of (d(s,t) - 1):
+    pinned on the golden graphs, so the GPU tests can use it at full size."""
+    for name, g in golden["graphs"].items():
+        offs, adj = _csr(g)
+        src = g["sources"] if g["sources"] is not None else list(range(g["n"]))
+        total = oracle.path_length_sum(offs, adj, src)
+        assert abs(sum(g["bc_half"]) * 2 - total) <= 1e-9 * max(total, 1), name
+    offs, adj = bcg.generate("rmat:scale=10,ef=8,seed=5,pendant_frac=0.1,pendant_mean=4")
+    src = bcg.sample_sources(len(offs) - 1, 200, 7)
+    bc, _ = oracle.bc(offs, adj, src, nthreads=4)
+    assert oracle.path_length_sum(offs, adj, src, nthreads=4) == pytest.approx(bc.sum(), rel=1e-12)
