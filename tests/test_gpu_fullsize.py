@@ -1,0 +1,66 @@
+"""GPU parity at the benchmark's full size (R-MAT scale 20 + pendant trees).
+
+Per-vertex comparison against the oracle on a sample of the benchmark's
+sources (the oracle finishes it in seconds), bit-exact levels and sigma for a
+few full-graph single-source runs, and for the whole 4096-source workload the
+size-independent identity sum_v bc[v] = sum_s sum_{t reachable} (d(s,t) - 1),
+whose right side needs only a BFS per source (pinned on the golden graphs in
+tests/test_oracle_golden.py)."""
+import numpy as np
+import pytest
+
+import bcg
+import oracle
+from test_gpu_parity import assert_bc_close
+
+pytestmark = pytest.mark.gpu
+
+SPEC = "rmat:scale=20,ef=16,a=0.57,b=0.19,c=0.19,seed=2,pendant_frac=0.1,pendant_mean=4"
+
+
+@pytest.fixture(scope="module")
+def big():
+    offs, adj = bcg.generate(SPEC)
+    src = bcg.sample_sources(len(offs) - 1, 4096, 2)
+    return offs, adj, src
+
+
+@pytest.mark.parametrize("width,flags", [(3, bcg.PRUNE_DEGREE1), (6, bcg.PRUNE_DEGREE1), (3, 0)])
+def test_sample_per_vertex(big, width, flags):
+    offs, adj, src = big
+    sample = src[:48]
+    ref, ost = oracle.bc(offs, adj, sample, nthreads=oracle.max_threads())
+    with bcg.Graph(offs, adj, flags) as G:
+        G.set_batch_width(width)
+        st = G.run(sample)
+        assert_bc_close(G.bc(), ref, f"s20 sample w={width} flags={flags}")
+        assert st.teps_edges == ost["teps_edges"]
+        assert st.skipped == ost["skipped"]
+
+
+def test_single_source_full_graph(big):
+    offs, adj, src = big
+    with bcg.Graph(offs, adj) as G:  # unpruned: every vertex gets a level
+        done = 0
+        for s in src:
+            if offs[s + 1] == offs[s]:
+                continue
+            lvl, sig, dl = G.single_source(int(s))
+            olvl, osig, odl, ov = oracle.single_source(offs, adj, int(s))
+            assert not ov
+            assert np.array_equal(lvl, olvl), s
+            assert np.array_equal(sig, osig), s
+            assert_bc_close(dl, odl, f"s20 delta s={s}")
+            done += 1
+            if done == 3:
+                break
+
+
+def test_workload_bc_total(big):
+    offs, adj, src = big
+    total = oracle.path_length_sum(offs, adj, src, nthreads=oracle.max_threads())
+    with bcg.Graph(offs, adj, bcg.PRUNE_DEGREE1) as G:
+        G.run(src)
+        bc = G.bc()
+    assert np.all(bc >= -1e-9)
+    assert abs(bc.sum() - total) <= 1e-9 * total, (bc.sum(), total)
