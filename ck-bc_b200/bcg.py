@@ -30,6 +30,10 @@ ERR_NOGPU = -9
 PRUNE_DEGREE1 = 0x1
 DIRECTED = 0x2
 
+NOALLOC_MAX_VERTICES = 65536
+NOALLOC_MAX_ADJ = 1048576
+NOALLOC_MAX_SOURCES = 65536
+
 _u32p = ctypes.POINTER(ctypes.c_uint32)
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _i32p = ctypes.POINTER(ctypes.c_int32)
@@ -93,6 +97,9 @@ SIGNATURES = {
     "bcg_run_weighted": (ctypes.c_int, [ctypes.c_void_p, _u32p, _f64p, _u32p, ctypes.c_uint64,
                                         ctypes.POINTER(Stats)]),
     "bcg_set_batch_width": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32]),
+    "bcg_bc_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64,
+                                      ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_int,
+                                      ctypes.c_void_p]),
     "bcg_last_error": (ctypes.c_char_p, []),
 }
 
@@ -252,6 +259,15 @@ class Graph:
 
     def set_batch_width(self, w: int):
         _check(lib().bcg_set_batch_width(self.h, w))
+
+
+def bc_noalloc(d_offsets: int, d_adj: int, n: int, nnz: int, d_sources: int, nsrc: int, d_bc: int,
+               accumulate: bool = False, stream: int = 0):
+    """bcg_bc_noalloc on raw device pointers (ints): exact BC of a device CSR
+    into the caller's device buffer d_bc[n], allocating no device memory."""
+    _check(lib().bcg_bc_noalloc(ctypes.c_void_p(d_offsets), ctypes.c_void_p(d_adj), n, nnz,
+                                ctypes.c_void_p(d_sources), nsrc, ctypes.c_void_p(d_bc), int(bool(accumulate)),
+                                ctypes.c_void_p(stream)))
 
 
 def bc_csr(offsets, adj, sources, flags: int = 0):

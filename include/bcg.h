@@ -201,6 +201,41 @@ int bcg_run_weighted(bcg_graph *g, const uint32_t *roots, const double *mult,
 /* Forces the sources-per-batch width (1, 3 or 6; 0 = automatic). */
 int bcg_set_batch_width(bcg_graph *g, uint32_t width);
 
+/* ---------------------------------------------------------------------------
+ * No-allocation entry point.  No counterpart in the reference: its
+ * cuda_kernels.cu allocates all device state in initcuda (cuda_kernels.cu:
+ * 1123-1198).  For callers that must not allocate device memory themselves
+ * or through a library: a framework whose own allocator owns the GPU's
+ * memory, or a latency-bound loop where cudaMalloc/cudaFree would
+ * synchronise the device.
+ * ------------------------------------------------------------------------ */
+
+#define BCG_NOALLOC_MAX_VERTICES 65536u    /* n */
+#define BCG_NOALLOC_MAX_ADJ      1048576u  /* nnz: adjacency entries (2 x undirected edges) */
+#define BCG_NOALLOC_MAX_SOURCES  65536u    /* sources per call */
+
+/* Exact BC of an undirected device-resident CSR (d_offsets[n+1], d_adj[nnz],
+ * lists as bcg_graph_create expects; no pruning) for the device-resident
+ * source list d_sources[nsrc] (degree-0 sources skipped, as bcg_run does),
+ * written into the caller's device buffer d_bc[n] (ordered-pair sums like
+ * bcg_get_bc): overwritten, or added to when accumulate != 0.  Work is
+ * enqueued on `stream` (a cudaStream_t, NULL = default stream); the call
+ * returns when it is done.
+ *   - Allocates no device memory and calls no allocating CUDA or library
+ *     function: all scratch lives in one fixed static device array of about
+ *     19 MiB per device, so n, nnz and nsrc are limited to the
+ *     BCG_NOALLOC_MAX_* values above; larger inputs return BCG_ERR_RANGE.
+ *   - The first call on each device (made with that device current) does the
+ *     setup: it takes the array's address with cudaGetSymbolAddress, which
+ *     loads the module.  Make that first call before any stream capture.
+ *   - One scratch per device: calls that overlap on the same device (other
+ *     threads or streams) race and must be serialised by the caller.
+ *   - Invalid CSR or source ids are found on the device before the sweep
+ *     runs and return BCG_ERR_ARG. */
+int bcg_bc_noalloc(const uint32_t *d_offsets, const uint32_t *d_adj, uint32_t n, uint64_t nnz,
+                   const uint32_t *d_sources, uint64_t nsrc, double *d_bc, int accumulate,
+                   void *stream);
+
 /* Message for the last error of the calling thread ("" if none). */
 const char *bcg_last_error(void);
 
