@@ -197,7 +197,7 @@ struct bcg_graph {
     std::vector<uint32_t> h_deg;     // original degree (source skip test)
     std::vector<uint32_t> h_anchor;  // empty when not pruned
     uint32_t forced_width = 0;
-    float ratio = 0.5f;
+    float ratio = 0.2f;
     unsigned long long wait_ns = kDefaultWaitNs;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };

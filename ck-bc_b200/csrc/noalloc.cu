@@ -377,7 +377,7 @@ extern "C" int bcg_bc_noalloc(const uint32_t *d_offsets, const uint32_t *d_adj, 
     a.ctrl = d_ctrl;
     a.rstat = reinterpret_cast<RootStat *>(scr + kOffRstat);
     a.nnz = nnz;
-    a.push_pull_ratio = 0.5f;
+    a.push_pull_ratio = 0.2f;
     if (const char *e = getenv("BCG_PUSH_PULL_RATIO")) a.push_pull_ratio = (float)atof(e);
     a.directed = 0;
     int grid = 0;
