@@ -97,6 +97,15 @@ SIGNATURES = {
     "bcg_run_weighted": (ctypes.c_int, [ctypes.c_void_p, _u32p, _f64p, _u32p, ctypes.c_uint64,
                                         ctypes.POINTER(Stats)]),
     "bcg_set_batch_width": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32]),
+    "bcg_batch_create": (ctypes.c_int, [ctypes.c_uint32, ctypes.POINTER(_u32p), ctypes.POINTER(_u32p), _u32p,
+                                        ctypes.POINTER(ctypes.c_void_p)]),
+    "bcg_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "bcg_batch_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Stats)]),
+    "bcg_batch_reset_bc": (ctypes.c_int, [ctypes.c_void_p]),
+    "bcg_batch_get_bc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, _f64p]),
+    "bcg_batch_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, _u32p, _u32p, _u32p]),
+    "bcg_batch_info": (ctypes.c_int, [ctypes.c_void_p, _u32p, _u32p, _u32p, _u32p,
+                                      ctypes.POINTER(ctypes.c_int)]),
     "bcg_bc_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64,
                                       ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_int,
                                       ctypes.c_void_p]),
@@ -259,6 +268,67 @@ class Graph:
 
     def set_batch_width(self, w: int):
         _check(lib().bcg_set_batch_width(self.h, w))
+
+
+class Batch:
+    """Many independent graphs resident as one disjoint union; run() adds every
+    graph's exact all-sources BC in one packed persistent launch."""
+
+    def __init__(self, graphs):
+        self._keep = [(np.ascontiguousarray(o, dtype=np.uint32), np.ascontiguousarray(a, dtype=np.uint32))
+                      for o, a in graphs]
+        k = len(self._keep)
+        self.sizes = [len(o) - 1 for o, _ in self._keep]
+        offs = (_u32p * k)(*[_p32(o) for o, _ in self._keep])
+        adjs = (_u32p * k)(*[_p32(a) if len(a) else None for _, a in self._keep])
+        n = np.array(self.sizes, dtype=np.uint32)
+        h = ctypes.c_void_p()
+        _check(lib().bcg_batch_create(k, offs, adjs, _p32(n), ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().bcg_batch_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self) -> Stats:
+        st = Stats()
+        _check(lib().bcg_batch_run(self.h, ctypes.byref(st)))
+        return st
+
+    def reset(self):
+        _check(lib().bcg_batch_reset_bc(self.h))
+
+    def bc(self, i: int) -> np.ndarray:
+        out = np.zeros(self.sizes[i], dtype=np.float64)
+        _check(lib().bcg_batch_get_bc(self.h, i, out.ctypes.data_as(_f64p)))
+        return out
+
+    def autotune(self, sample_batches: int = 0):
+        w, tv, te = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        _check(lib().bcg_batch_autotune(self.h, sample_batches, ctypes.byref(w), ctypes.byref(tv),
+                                        ctypes.byref(te)))
+        return w.value, tv.value, te.value
+
+    def info(self):
+        nb, w, tv, te = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        cap = ctypes.c_int()
+        _check(lib().bcg_batch_info(self.h, ctypes.byref(nb), ctypes.byref(w), ctypes.byref(tv), ctypes.byref(te),
+                                    ctypes.byref(cap)))
+        return {"nbatch": nb.value, "width": w.value, "tile_vertices": tv.value, "tile_entries": te.value,
+                "captured": bool(cap.value)}
 
 
 def bc_noalloc(d_offsets: int, d_adj: int, n: int, nnz: int, d_sources: int, nsrc: int, d_bc: int,

@@ -1,0 +1,397 @@
+// Batched form: exact all-sources BC of many independent graphs in one
+// persistent launch (no counterpart in the reference, whose program runs one
+// graph per process; the per-graph computation is the same as bcg_run's).
+//
+// The graphs are laid out on the device as one disjoint union (graph g's
+// vertex v is union vertex base[g] + v), ordered by their count of
+// non-isolated vertices, largest first.  Brandes on a disjoint union is Brandes
+// on each component, so each graph's slice of the union's bc is that graph's
+// bc.  Sources are packed per component: batch i puts, in slot k, the
+// (i*S + k)-th non-isolated vertex of every graph that has that many, so one
+// batch advances every active graph at once and the sweeps of small graphs
+// share the grid barriers of the large ones.  Graphs still active in batch i
+// are a prefix of the union, so the first pull of the batch walks only the
+// tiles of that prefix.  The whole schedule runs in one cooperative launch,
+// captured once into a CUDA graph and replayed by every bcg_batch_run.
+//
+// The autotuner times a prefix of the schedule for each candidate batch width
+// S in {1, 3, 6} and tile shape (vertices x adjacency entries per tile), keeps
+// the fastest per root, and rebuilds the schedule for it.
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "bcg_common.hpp"
+#include "engine_internal.hpp"
+
+using namespace bcg;
+
+struct bcg_batch {
+    bcg_graph *g = nullptr;
+    uint32_t ngraphs = 0;
+    std::vector<uint32_t> base, gn;  // per caller graph: first union vertex, vertex count
+    std::vector<uint32_t> order;     // union position -> caller graph
+    std::vector<uint32_t> hdeg;      // union degrees
+    uint32_t width = 3;
+    // device schedule of the current width and tile shape
+    uint32_t *d_xbeg = nullptr, *d_xroots = nullptr, *d_xtiles = nullptr;
+    unsigned char *d_xslot = nullptr;
+    unsigned long long *d_xpf = nullptr, *d_xpu = nullptr;
+    RootStat *d_rstat = nullptr;
+    uint32_t nbatch = 0;
+    uint64_t nroots = 0;
+    std::vector<uint32_t> hxbeg;  // host copy of the batch starts
+    cudaStream_t stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int captured = 0;  // 1: runs replay a captured CUDA graph; 0: direct launches
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+#define CKB(call)                                                                                  \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return set_error(e_ == cudaErrorMemoryAllocation ? BCG_ERR_OOM : BCG_ERR_CUDA, "%s failed: %s", \
+                             #call, cudaGetErrorString(e_));                                       \
+    } while (0)
+
+void free_schedule(bcg_batch *b) {
+    cudaFree(b->d_xbeg); cudaFree(b->d_xroots); cudaFree(b->d_xtiles); cudaFree(b->d_xslot);
+    cudaFree(b->d_xpf); cudaFree(b->d_xpu); cudaFree(b->d_rstat);
+    b->d_xbeg = b->d_xroots = b->d_xtiles = nullptr;
+    b->d_xslot = nullptr;
+    b->d_xpf = b->d_xpu = nullptr;
+    b->d_rstat = nullptr;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    b->captured = 0;
+}
+
+// Builds and uploads the packed schedule for width b->width and the graph's
+// current tiles.
+int build_schedule(bcg_batch *b) {
+    free_schedule(b);
+    const uint32_t S = b->width;
+    bcg_graph *g = b->g;
+    std::vector<uint32_t> tile_of(g->n);
+    CKB(cudaMemcpy(tile_of.data(), g->d_tile_of, (size_t)g->n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    // per union position: its non-isolated vertices, and the graph's entries
+    const uint32_t G = b->ngraphs;
+    std::vector<std::vector<uint32_t>> act(G);
+    std::vector<uint64_t> gnnz(G, 0);
+    uint32_t maxc = 0;
+    for (uint32_t p = 0; p < G; ++p) {
+        const uint32_t gi = b->order[p];
+        const uint32_t v0 = b->base[gi], nv = b->gn[gi];
+        for (uint32_t v = v0; v < v0 + nv; ++v) {
+            gnnz[p] += b->hdeg[v];
+            if (b->hdeg[v]) act[p].push_back(v);
+        }
+        maxc = std::max<uint32_t>(maxc, (uint32_t)act[p].size());
+    }
+    const uint32_t nb = (maxc + S - 1) / S;
+    std::vector<uint32_t> xbeg(nb + 1, 0), xroots, xtiles(nb);
+    std::vector<unsigned char> xslot;
+    std::vector<unsigned long long> xpf(nb, 0), xpu(nb, 0);
+    for (uint32_t i = 0; i < nb; ++i) {
+        uint32_t last_active = 0;  // union positions [0, last_active) have roots in batch i
+        for (uint32_t p = 0; p < G; ++p) {
+            if (act[p].size() <= (size_t)i * S) break;  // sorted: no later graph is active
+            last_active = p + 1;
+            for (uint32_t k = 0; k < S; ++k) {
+                const size_t j = (size_t)i * S + k;
+                if (j >= act[p].size()) break;
+                const uint32_t r = act[p][j];
+                xroots.push_back(r);
+                xslot.push_back((unsigned char)k);
+                xpf[i] += b->hdeg[r];
+                xpu[i] += gnnz[p] - b->hdeg[r];
+            }
+        }
+        xbeg[i + 1] = (uint32_t)xroots.size();
+        // tiles of the active prefix: up to and including the tile of the first
+        // vertex past it (a tile may straddle two graphs)
+        if (last_active >= G) {
+            xtiles[i] = g->ntiles;
+        } else {
+            const uint32_t v_end = b->base[b->order[last_active]];
+            xtiles[i] = std::min(g->ntiles, (tile_of[v_end] & ~kHubFlag) + 1);
+        }
+    }
+    b->nbatch = nb;
+    b->nroots = xroots.size();
+    b->hxbeg = xbeg;
+    if (nb == 0) return BCG_OK;
+    CKB(cudaMalloc(&b->d_xbeg, xbeg.size() * sizeof(uint32_t)));
+    CKB(cudaMalloc(&b->d_xroots, std::max<size_t>(1, xroots.size()) * sizeof(uint32_t)));
+    CKB(cudaMalloc(&b->d_xslot, std::max<size_t>(1, xslot.size())));
+    CKB(cudaMalloc(&b->d_xtiles, nb * sizeof(uint32_t)));
+    CKB(cudaMalloc(&b->d_xpf, nb * sizeof(unsigned long long)));
+    CKB(cudaMalloc(&b->d_xpu, nb * sizeof(unsigned long long)));
+    CKB(cudaMalloc(&b->d_rstat, (size_t)nb * S * sizeof(RootStat)));
+    CKB(cudaMemcpy(b->d_xbeg, xbeg.data(), xbeg.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    if (!xroots.empty()) {
+        CKB(cudaMemcpy(b->d_xroots, xroots.data(), xroots.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+        CKB(cudaMemcpy(b->d_xslot, xslot.data(), xslot.size(), cudaMemcpyHostToDevice));
+    }
+    CKB(cudaMemcpy(b->d_xtiles, xtiles.data(), nb * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    CKB(cudaMemcpy(b->d_xpf, xpf.data(), nb * sizeof(unsigned long long), cudaMemcpyHostToDevice));
+    CKB(cudaMemcpy(b->d_xpu, xpu.data(), nb * sizeof(unsigned long long), cudaMemcpyHostToDevice));
+    return ensure_state(g, S);
+}
+
+PackedRun packed_prefix(const bcg_batch *b, uint32_t nbatch) {
+    PackedRun p{};
+    p.xbeg = b->d_xbeg;
+    p.xroots = b->d_xroots;
+    p.xslot = b->d_xslot;
+    p.xpf = b->d_xpf;
+    p.xpu = b->d_xpu;
+    p.xtiles = b->d_xtiles;
+    p.nbatch = nbatch;
+    p.rstat = b->d_rstat;
+    return p;
+}
+
+// One run of the first nbatch batches on b->stream, timed with events.
+int timed_run(bcg_batch *b, uint32_t nbatch, float *ms) {
+    CKB(cudaEventRecord(b->ev0, b->stream));
+    int rc = enqueue_packed(b->g, packed_prefix(b, nbatch), b->width, b->stream);
+    if (rc) return rc;
+    CKB(cudaEventRecord(b->ev1, b->stream));
+    rc = check_ctrl(b->g, b->stream);
+    if (rc) return rc;
+    CKB(cudaEventElapsedTime(ms, b->ev0, b->ev1));
+    return BCG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bcg_batch_create(uint32_t ngraphs, const uint32_t *const *offsets, const uint32_t *const *adj,
+                     const uint32_t *n, bcg_batch **out) {
+    clear_error();
+    if (!out) return set_error(BCG_ERR_ARG, "null output handle");
+    *out = nullptr;
+    if (ngraphs == 0 || !offsets || !adj || !n) return set_error(BCG_ERR_ARG, "no graphs or null arrays");
+    uint64_t N = 0, NNZ = 0;
+    for (uint32_t i = 0; i < ngraphs; ++i) {
+        if (!offsets[i] || n[i] == 0) return set_error(BCG_ERR_ARG, "graph %u: null offsets or n == 0", i);
+        if (offsets[i][n[i]] && !adj[i]) return set_error(BCG_ERR_ARG, "graph %u: null adjacency", i);
+        N += n[i];
+        NNZ += offsets[i][n[i]];
+    }
+    if (N > 0xFFFFFFFEull || NNZ > 0xFFFFFFFFull)
+        return set_error(BCG_ERR_RANGE, "union of %u graphs exceeds 32-bit ids/offsets", ngraphs);
+    bcg_batch *b = new bcg_batch();
+    b->ngraphs = ngraphs;
+    b->base.resize(ngraphs);
+    b->gn.assign(n, n + ngraphs);
+    // union order: most non-isolated vertices first
+    std::vector<uint32_t> act(ngraphs, 0);
+    for (uint32_t i = 0; i < ngraphs; ++i)
+        for (uint32_t v = 0; v < n[i]; ++v) act[i] += (offsets[i][v + 1] > offsets[i][v]);
+    b->order.resize(ngraphs);
+    std::iota(b->order.begin(), b->order.end(), 0u);
+    std::stable_sort(b->order.begin(), b->order.end(), [&](uint32_t x, uint32_t y) { return act[x] > act[y]; });
+    std::vector<uint32_t> uoffs(N + 1), uadj(NNZ);
+    b->hdeg.resize(N);
+    uint64_t vpos = 0, epos = 0;
+    for (uint32_t p = 0; p < ngraphs; ++p) {
+        const uint32_t gi = b->order[p];
+        const uint32_t vb = (uint32_t)vpos;
+        b->base[gi] = vb;
+        const uint32_t *o = offsets[gi];
+        for (uint32_t v = 0; v < n[gi]; ++v) {
+            uoffs[vpos] = (uint32_t)epos;
+            b->hdeg[vpos] = o[v + 1] - o[v];
+            for (uint32_t e = o[v]; e < o[v + 1]; ++e) {
+                const uint32_t w = adj[gi][e];
+                if (w >= n[gi]) {
+                    delete b;
+                    return set_error(BCG_ERR_ARG, "graph %u: adj[%u] = %u >= n=%u", gi, e, w, n[gi]);
+                }
+                uadj[epos++] = vb + w;
+            }
+            ++vpos;
+        }
+    }
+    uoffs[N] = (uint32_t)epos;
+    int rc = bcg_graph_create(uoffs.data(), uadj.data(), (uint32_t)N, NNZ, 0, &b->g);
+    if (rc) {
+        delete b;
+        return rc;
+    }
+    auto fail = [&](int code) {
+        bcg_batch_destroy(b);
+        return code;
+    };
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreate(&b->ev0)) != cudaSuccess || (e = cudaEventCreate(&b->ev1)) != cudaSuccess)
+        return fail(set_error(BCG_ERR_CUDA, "stream/event: %s", cudaGetErrorString(e)));
+    rc = build_schedule(b);
+    if (rc) return fail(rc);
+    *out = b;
+    return BCG_OK;
+}
+
+int bcg_batch_destroy(bcg_batch *b) {
+    clear_error();
+    if (!b) return set_error(BCG_ERR_ARG, "null handle");
+    free_schedule(b);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    if (b->g) bcg_graph_destroy(b->g);
+    delete b;
+    return BCG_OK;
+}
+
+int bcg_batch_run(bcg_batch *b, bcg_stats *stats) {
+    clear_error();
+    if (!b) return set_error(BCG_ERR_ARG, "null handle");
+    if (stats) *stats = bcg_stats{};
+    if (b->nbatch) {
+        if (!b->exec) {
+            // capture the whole packed launch once; if the capture cannot be
+            // made, runs launch directly (b->captured says which)
+            cudaGraph_t graph = nullptr;
+            int rc = BCG_ERR_CUDA;
+            if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed) == cudaSuccess) {
+                rc = enqueue_packed(b->g, packed_prefix(b, b->nbatch), b->width, b->stream);
+                const cudaError_t ee = cudaStreamEndCapture(b->stream, &graph);
+                if (rc == BCG_OK && ee == cudaSuccess && graph &&
+                    cudaGraphInstantiate(&b->exec, graph, 0) == cudaSuccess) {
+                    b->graph = graph;
+                    b->captured = 1;
+                } else {
+                    if (graph) cudaGraphDestroy(graph);
+                    b->exec = nullptr;
+                }
+            }
+            cudaGetLastError();  // a refused capture leaves no sticky error
+            clear_error();
+        }
+        CKB(cudaEventRecord(b->ev0, b->stream));
+        if (b->exec) {
+            CKB(cudaGraphLaunch(b->exec, b->stream));
+        } else {
+            const int rc = enqueue_packed(b->g, packed_prefix(b, b->nbatch), b->width, b->stream);
+            if (rc) return rc;
+        }
+        CKB(cudaEventRecord(b->ev1, b->stream));
+        const int rc = check_ctrl(b->g, b->stream);
+        if (rc) return rc;
+    }
+    if (stats) {
+        const uint32_t S = b->width;
+        std::vector<RootStat> rs((size_t)b->nbatch * S);
+        if (!rs.empty())
+            CKB(cudaMemcpy(rs.data(), b->d_rstat, rs.size() * sizeof(RootStat), cudaMemcpyDeviceToHost));
+        uint64_t teps = 0, vis = 0, cv = 0;
+        uint32_t md = 0;
+        for (const RootStat &r : rs) {
+            teps += r.mc2 / 2;
+            vis += r.visited;
+            cv += r.wsum;
+            md = std::max(md, r.depth);
+        }
+        uint64_t nsrc = 0;
+        for (uint32_t i = 0; i < b->ngraphs; ++i) nsrc += b->gn[i];
+        float ms = 0.f;
+        if (b->nbatch) cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+        stats->sources = nsrc;
+        stats->roots = b->nroots;
+        stats->skipped = nsrc - b->nroots;
+        stats->batches = b->nbatch;
+        stats->teps_edges = teps;
+        stats->visited = vis;
+        stats->comp_vertices = cv;
+        stats->max_depth = md;
+        stats->batch_width = S;
+        stats->kernel_ms = ms;
+    }
+    return BCG_OK;
+}
+
+int bcg_batch_reset_bc(bcg_batch *b) {
+    clear_error();
+    if (!b) return set_error(BCG_ERR_ARG, "null handle");
+    return bcg_reset_bc(b->g);
+}
+
+int bcg_batch_get_bc(bcg_batch *b, uint32_t graph, double *bc_host) {
+    clear_error();
+    if (!b || !bc_host) return set_error(BCG_ERR_ARG, "null argument");
+    if (graph >= b->ngraphs) return set_error(BCG_ERR_ARG, "graph %u >= %u graphs", graph, b->ngraphs);
+    double *d_bc = nullptr;
+    int rc = bcg_bc_device_ptr(b->g, &d_bc);
+    if (rc) return rc;
+    CKB(cudaMemcpy(bc_host, d_bc + b->base[graph], (size_t)b->gn[graph] * sizeof(double), cudaMemcpyDeviceToHost));
+    return BCG_OK;
+}
+
+int bcg_batch_autotune(bcg_batch *b, uint32_t sample_batches, uint32_t *width, uint32_t *tile_vertices,
+                       uint32_t *tile_entries) {
+    clear_error();
+    if (!b) return set_error(BCG_ERR_ARG, "null handle");
+    static const uint32_t widths[] = {1, 3, 6};
+    static const uint32_t shapes[][2] = {{32, 256}, {32, 128}, {16, 128}, {16, 64}};
+    double best = 0.0;
+    uint32_t bw = b->width, bv = b->g->tile_vcap, be = b->g->tile_ecap;
+    for (const auto &sh : shapes) {
+        int rc = graph_retile(b->g, sh[0], sh[1]);
+        if (rc) return rc;
+        for (uint32_t S : widths) {
+            b->width = S;
+            rc = build_schedule(b);
+            if (rc) return rc;
+            if (!b->nbatch) continue;
+            const uint32_t nb = std::max(1u, std::min(b->nbatch, sample_batches ? sample_batches : 4u));
+            float ms = 0.f;
+            rc = timed_run(b, nb, &ms);  // warm-up (module, state, caches)
+            if (!rc) rc = timed_run(b, nb, &ms);
+            if (rc) return rc;
+            const double per_root = ms / std::max<uint32_t>(1, b->hxbeg[nb]);
+            if (best == 0.0 || per_root < best) {
+                best = per_root;
+                bw = S;
+                bv = sh[0];
+                be = sh[1];
+            }
+        }
+    }
+    int rc = graph_retile(b->g, bv, be);
+    if (rc) return rc;
+    b->width = bw;
+    rc = build_schedule(b);
+    if (rc) return rc;
+    rc = bcg_reset_bc(b->g);  // the timing runs added into the accumulators
+    if (rc) return rc;
+    if (width) *width = bw;
+    if (tile_vertices) *tile_vertices = bv;
+    if (tile_entries) *tile_entries = be;
+    return BCG_OK;
+}
+
+int bcg_batch_info(bcg_batch *b, uint32_t *nbatch, uint32_t *width, uint32_t *tile_vertices,
+                   uint32_t *tile_entries, int *captured) {
+    clear_error();
+    if (!b) return set_error(BCG_ERR_ARG, "null handle");
+    if (nbatch) *nbatch = b->nbatch;
+    if (width) *width = b->width;
+    if (tile_vertices) *tile_vertices = b->g->tile_vcap;
+    if (tile_entries) *tile_entries = b->g->tile_ecap;
+    if (captured) *captured = b->captured;
+    return BCG_OK;
+}
+
+}  // extern "C"

@@ -35,10 +35,10 @@
 
 #include "bcg_common.hpp"
 #include "engine.cuh"
+#include "engine_internal.hpp"
 
 namespace bcg {
 
-int launch_sweep(int S, const BatchArgs &a, cudaStream_t st, int *grid_out);
 
 #define CK(call)                                                                           \
     do {                                                                                   \
@@ -121,24 +121,27 @@ __global__ void k_levels_out(uint32_t n, const unsigned char *__restrict__ rows,
 // Work tiles (host, from the original row starts).
 // ---------------------------------------------------------------------------
 
+// Runs of at most vcap consecutive vertices with at most ecap adjacency
+// entries; a vertex with more than ecap entries is split into ecap-entry
+// chunks (vcap <= 32, ecap <= 256: the sweep kernel's lane and run limits).
 // tile_of[v] = index of v's tile (of its first chunk, with kHubFlag, when v
 // is split).
-static void build_tiles(const uint32_t *offs, uint32_t n, std::vector<Tile> &tiles, uint32_t &nhub,
-                        std::vector<uint32_t> &tile_of) {
+static void build_tiles(const uint32_t *offs, uint32_t n, uint32_t vcap, uint32_t ecap, std::vector<Tile> &tiles,
+                        uint32_t &nhub, std::vector<uint32_t> &tile_of) {
     tiles.clear();
     tile_of.assign(n, 0);
     nhub = 0;
     uint32_t v = 0;
     while (v < n) {
         const uint32_t dv = offs[v + 1] - offs[v];
-        if (dv > (uint32_t)kTileEdges) {
-            const uint32_t nch = (dv + kTileEdges - 1) / kTileEdges;
+        if (dv > ecap) {
+            const uint32_t nch = (dv + ecap - 1) / ecap;
             tile_of[v] = (uint32_t)tiles.size() | kHubFlag;
             for (uint32_t c = 0; c < nch; ++c) {
                 Tile t{};
                 t.v0 = v; t.v1 = v + 1;
-                t.e0 = offs[v] + c * kTileEdges;
-                t.e1 = std::min(offs[v + 1], t.e0 + (uint32_t)kTileEdges);
+                t.e0 = offs[v] + c * ecap;
+                t.e1 = std::min(offs[v + 1], t.e0 + ecap);
                 t.hub = (int32_t)nhub;
                 t.nchunks = nch;
                 tiles.push_back(t);
@@ -149,9 +152,9 @@ static void build_tiles(const uint32_t *offs, uint32_t n, std::vector<Tile> &til
         }
         const uint32_t start = v;
         uint32_t sum = 0;
-        while (v < n && v - start < (uint32_t)kTileVerts) {
+        while (v < n && v - start < vcap) {
             const uint32_t d = offs[v + 1] - offs[v];
-            if (d > (uint32_t)kTileEdges || sum + d > (uint32_t)kTileEdges) break;
+            if (d > ecap || sum + d > ecap) break;
             sum += d;
             tile_of[v] = (uint32_t)tiles.size();
             ++v;
@@ -169,38 +172,6 @@ static void build_tiles(const uint32_t *offs, uint32_t n, std::vector<Tile> &til
 
 using namespace bcg;
 
-struct bcg_graph {
-    int device = 0;
-    uint32_t n = 0;
-    uint64_t nnz = 0, nnz_pruned = 0;
-    uint32_t flags = 0;
-    uint32_t npruned = 0;
-    uint32_t *d_offs = nullptr, *d_adj = nullptr;
-    uint2 *d_vinfo = nullptr;
-    uint32_t *d_anchor = nullptr, *d_reach = nullptr;
-    double *d_bc = nullptr;
-    Tile *d_tiles = nullptr;
-    uint32_t ntiles = 0, nhub = 0;
-    unsigned long long *d_hub_acc = nullptr;
-    unsigned int *d_hub_cnt = nullptr;
-    uint32_t *d_tile_of = nullptr, *d_tmark = nullptr;
-    uint32_t *d_lists = nullptr, *d_lbase = nullptr, *d_lcnt = nullptr;
-    uint32_t *d_ulist = nullptr;  // ring of 2 * ntiles (tiles with unvisited vertices)
-    unsigned long long list_cap = 0;
-    unsigned char *d_rows = nullptr;  // n state rows of row_bytes(state_width)
-    uint32_t state_width = 0;
-    Ctrl *d_ctrl = nullptr;
-    uint32_t *d_roots = nullptr, *d_pend = nullptr;
-    double *d_mult = nullptr;
-    RootStat *d_rstat = nullptr;
-    size_t run_cap = 0;
-    std::vector<uint32_t> h_deg;     // original degree (source skip test)
-    std::vector<uint32_t> h_anchor;  // empty when not pruned
-    uint32_t forced_width = 0;
-    float ratio = 0.2f;
-    unsigned long long wait_ns = kDefaultWaitNs;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-};
 
 namespace bcg {
 
@@ -222,7 +193,7 @@ static void graph_free(bcg_graph *g) {
     delete g;
 }
 
-static int ensure_state(bcg_graph *g, uint32_t S) {
+int ensure_state(bcg_graph *g, uint32_t S) {
     if (g->state_width >= S) return BCG_OK;  // row_bytes grows with S
     cudaFree(g->d_rows); g->d_rows = nullptr;
     cudaFree(g->d_hub_acc); g->d_hub_acc = nullptr;
@@ -267,6 +238,25 @@ static uint32_t choose_width(const bcg_graph *g, uint64_t nroots) {
     return S;
 }
 
+// Work tiles of the current shape and the per-tile buffers.
+static int setup_tiles(bcg_graph *g, const uint32_t *h_offs) {
+    const uint32_t n = g->n;
+    std::vector<Tile> tiles;
+    std::vector<uint32_t> tile_of;
+    build_tiles(h_offs, n, g->tile_vcap, g->tile_ecap, tiles, g->nhub, tile_of);
+    g->ntiles = (uint32_t)tiles.size();
+    CK(cudaMalloc(&g->d_tiles, std::max<size_t>(1, tiles.size()) * sizeof(Tile)));
+    if (!tiles.empty())
+        CK(cudaMemcpy(g->d_tiles, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&g->d_tile_of, (size_t)n * sizeof(uint32_t)));
+    CK(cudaMemcpy(g->d_tile_of, tile_of.data(), (size_t)n * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&g->d_tmark, std::max<size_t>(1, tiles.size()) * sizeof(uint32_t)));
+    CK(cudaMalloc(&g->d_ulist, 2 * std::max<size_t>(1, tiles.size()) * sizeof(uint32_t)));
+    CK(cudaMalloc(&g->d_hub_cnt, (size_t)std::max(1u, g->nhub) * sizeof(unsigned int)));
+    CK(cudaMemset(g->d_hub_cnt, 0, (size_t)std::max(1u, g->nhub) * sizeof(unsigned int)));
+    return BCG_OK;
+}
+
 static int create_common(bcg_graph *g, const uint32_t *h_offs) {
     const uint32_t n = g->n;
     CK(cudaMalloc(&g->d_vinfo, (size_t)n * sizeof(uint2)));
@@ -300,23 +290,29 @@ static int create_common(bcg_graph *g, const uint32_t *h_offs) {
         CK(cudaGetLastError());
         g->nnz_pruned = g->nnz;
     }
-    std::vector<Tile> tiles;
-    std::vector<uint32_t> tile_of;
-    build_tiles(h_offs, n, tiles, g->nhub, tile_of);
-    g->ntiles = (uint32_t)tiles.size();
-    CK(cudaMalloc(&g->d_tiles, std::max<size_t>(1, tiles.size()) * sizeof(Tile)));
-    if (!tiles.empty())
-        CK(cudaMemcpy(g->d_tiles, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice));
-    CK(cudaMalloc(&g->d_tile_of, (size_t)n * sizeof(uint32_t)));
-    CK(cudaMemcpy(g->d_tile_of, tile_of.data(), (size_t)n * sizeof(uint32_t), cudaMemcpyHostToDevice));
-    CK(cudaMalloc(&g->d_tmark, std::max<size_t>(1, tiles.size()) * sizeof(uint32_t)));
     CK(cudaMalloc(&g->d_lbase, (size_t)(kMaxLevel + 3) * sizeof(uint32_t)));
     CK(cudaMalloc(&g->d_lcnt, (size_t)(kMaxLevel + 3) * sizeof(uint32_t)));
-    CK(cudaMalloc(&g->d_ulist, 2 * std::max<size_t>(1, tiles.size()) * sizeof(uint32_t)));
-    CK(cudaMalloc(&g->d_hub_cnt, (size_t)std::max(1u, g->nhub) * sizeof(unsigned int)));
-    CK(cudaMemset(g->d_hub_cnt, 0, (size_t)std::max(1u, g->nhub) * sizeof(unsigned int)));
+    const int rc = setup_tiles(g, h_offs);
+    if (rc) return rc;
     CK(cudaDeviceSynchronize());
     return BCG_OK;
+}
+
+int graph_retile(bcg_graph *g, uint32_t vcap, uint32_t ecap) {
+    if (vcap < 1 || vcap > (uint32_t)kTileVerts || ecap < 1 || ecap > (uint32_t)kTileEdges)
+        return set_error(BCG_ERR_ARG, "tile shape %ux%u outside 1..%d vertices, 1..%d entries", vcap, ecap,
+                         kTileVerts, kTileEdges);
+    if (vcap == g->tile_vcap && ecap == g->tile_ecap) return BCG_OK;
+    std::vector<uint32_t> h_offs((size_t)g->n + 1);
+    CK(cudaMemcpy(h_offs.data(), g->d_offs, h_offs.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    cudaFree(g->d_tiles); cudaFree(g->d_tile_of); cudaFree(g->d_tmark); cudaFree(g->d_ulist);
+    cudaFree(g->d_hub_cnt); cudaFree(g->d_hub_acc); cudaFree(g->d_lists);
+    g->d_tiles = nullptr; g->d_tile_of = g->d_tmark = g->d_ulist = g->d_lists = nullptr;
+    g->d_hub_cnt = nullptr; g->d_hub_acc = nullptr;
+    g->state_width = 0;  // hub accumulators and lists are sized by the tiles
+    g->tile_vcap = vcap;
+    g->tile_ecap = ecap;
+    return setup_tiles(g, h_offs.data());
 }
 
 static int check_device() {
@@ -500,6 +496,66 @@ static int run_plan(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *
         stats->batch_width = S;
         stats->kernel_ms = ms;
     }
+    return BCG_OK;
+}
+
+// BatchArgs fields common to every launch on g.
+static void fill_args(bcg_graph *g, BatchArgs &a) {
+    a.n = g->n;
+    a.offs = g->d_offs;
+    a.adj = g->d_adj;
+    a.vinfo = g->d_vinfo;
+    a.tiles = g->d_tiles;
+    a.ntiles = g->ntiles;
+    a.tile_of = g->d_tile_of;
+    a.tmark = g->d_tmark;
+    a.lists = g->d_lists;
+    a.list_cap = g->list_cap;
+    a.ulist = g->d_ulist;
+    a.lbase = g->d_lbase;
+    a.lcnt = g->d_lcnt;
+    a.rows = g->d_rows;
+    a.bc = g->d_bc;
+    a.hub_acc = g->d_hub_acc;
+    a.hub_cnt = g->d_hub_cnt;
+    a.ctrl = g->d_ctrl;
+    a.nnz = g->nnz_pruned;
+    a.push_pull_ratio = g->ratio;
+    a.directed = (g->flags & BCG_DIRECTED) ? 1 : 0;
+}
+
+int enqueue_packed(bcg_graph *g, const PackedRun &p, uint32_t S, cudaStream_t st) {
+    if (p.nbatch == 0) return BCG_OK;
+    // tile marks key on the batch index modulo 2^16 (one launch, <= 65535 batches)
+    if (p.nbatch > 65535) return set_error(BCG_ERR_RANGE, "%u packed batches exceed one launch (65535)", p.nbatch);
+    int rc = ensure_state(g, S);
+    if (rc) return rc;
+    const size_t nh = std::max(1u, g->nhub);
+    CK(cudaMemsetAsync(g->d_hub_acc, 0, nh * S * sizeof(unsigned long long), st));
+    CK(cudaMemsetAsync(g->d_hub_cnt, 0, nh * sizeof(unsigned int), st));
+    CK(cudaMemsetAsync(g->d_ctrl, 0, sizeof(Ctrl), st));  // wait bound 0: the kernel's default
+    CK(cudaMemsetAsync(g->d_tmark, 0, (size_t)std::max(1u, g->ntiles) * sizeof(uint32_t), st));
+    BatchArgs a{};
+    fill_args(g, a);
+    a.rstat = p.rstat;
+    a.nbatch = p.nbatch;
+    a.xbeg = p.xbeg;
+    a.xroots = p.xroots;
+    a.xslot = p.xslot;
+    a.xpf = p.xpf;
+    a.xpu = p.xpu;
+    a.xtiles = p.xtiles;
+    int grid = 0;
+    return launch_sweep((int)S, a, st, &grid);
+}
+
+int check_ctrl(bcg_graph *g, cudaStream_t st) {
+    CK(cudaStreamSynchronize(st));
+    Ctrl c{};
+    CK(cudaMemcpy(&c, g->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+    if (c.error) return set_error(c.error, "device reported error %d (%s)", c.error,
+                                  c.error == BCG_ERR_TIMEOUT ? "a bounded wait gave up" : "level limit exceeded");
+    if (c.overflow) return set_error(BCG_ERR_OVERFLOW, "a shortest-path count exceeded 2^64");
     return BCG_OK;
 }
 

@@ -127,6 +127,21 @@ struct BatchArgs {
     TraceRec *trace;
     unsigned int trace_cap;
     unsigned int *trace_cnt;
+    // Component-packed batches (xbeg == nullptr: one root per slot, given by
+    // roots / mult / pend).  Batch b runs roots xroots[xbeg[b] .. xbeg[b+1]),
+    // root i in slot xslot[i]; roots that share a slot lie in different
+    // connected components, so their searches never meet.  Every such root has
+    // weight 1 and no pendant sources; the per-slot counters add up over its
+    // roots.  xpu[b] = sum over the batch's roots of the adjacency entries of
+    // their components minus their own degrees (level 0's unvisited
+    // pair-edges); the first xtiles[b] tiles hold every vertex of those
+    // components (the first pull of the batch walks only them).
+    const uint32_t *xbeg;
+    const uint32_t *xroots;
+    const unsigned char *xslot;
+    const unsigned long long *xpf;   // per batch: sum of the roots' degrees
+    const unsigned long long *xpu;
+    const uint32_t *xtiles;
 };
 
 }  // namespace bcg

@@ -1,0 +1,75 @@
+// Host-side state of one graph on the device, shared by the engine's
+// translation units (engine.cu: single graphs; batch.cu: packed unions of
+// graphs).  Not part of the public ABI.
+#pragma once
+#include <vector>
+
+#include "bcg.h"
+#include "engine.cuh"
+
+using bcg::Ctrl;
+using bcg::RootStat;
+using bcg::Tile;
+using bcg::kDefaultWaitNs;
+using bcg::kTileEdges;
+using bcg::kTileVerts;
+
+struct bcg_graph {
+    int device = 0;
+    uint32_t n = 0;
+    uint64_t nnz = 0, nnz_pruned = 0;
+    uint32_t flags = 0;
+    uint32_t npruned = 0;
+    uint32_t *d_offs = nullptr, *d_adj = nullptr;
+    uint2 *d_vinfo = nullptr;
+    uint32_t *d_anchor = nullptr, *d_reach = nullptr;
+    double *d_bc = nullptr;
+    Tile *d_tiles = nullptr;
+    uint32_t ntiles = 0, nhub = 0;
+    unsigned long long *d_hub_acc = nullptr;
+    unsigned int *d_hub_cnt = nullptr;
+    uint32_t *d_tile_of = nullptr, *d_tmark = nullptr;
+    uint32_t *d_lists = nullptr, *d_lbase = nullptr, *d_lcnt = nullptr;
+    uint32_t *d_ulist = nullptr;  // ring of 2 * ntiles (tiles with unvisited vertices)
+    unsigned long long list_cap = 0;
+    unsigned char *d_rows = nullptr;  // n state rows of row_bytes(state_width)
+    uint32_t state_width = 0;
+    Ctrl *d_ctrl = nullptr;
+    uint32_t *d_roots = nullptr, *d_pend = nullptr;
+    double *d_mult = nullptr;
+    RootStat *d_rstat = nullptr;
+    size_t run_cap = 0;
+    std::vector<uint32_t> h_deg;     // original degree (source skip test)
+    std::vector<uint32_t> h_anchor;  // empty when not pruned
+    uint32_t forced_width = 0;
+    uint32_t tile_vcap = kTileVerts, tile_ecap = kTileEdges;  // tile shape (autotuned by batches)
+    float ratio = 0.2f;
+    unsigned long long wait_ns = kDefaultWaitNs;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace bcg {
+
+int launch_sweep(int S, const BatchArgs &a, cudaStream_t st, int *grid_out);
+
+// Component-packed batches already on the device (see BatchArgs::xbeg).
+struct PackedRun {
+    const uint32_t *xbeg, *xroots;
+    const unsigned char *xslot;
+    const unsigned long long *xpf, *xpu;
+    const uint32_t *xtiles;
+    uint32_t nbatch;
+    RootStat *rstat;  // nbatch * S per-slot totals
+};
+
+// Grows the state rows, hub accumulators and level lists for width S.
+int ensure_state(bcg_graph *g, uint32_t S);
+// Enqueues one packed launch on st (memsets + the sweep kernel; no host
+// synchronisation, so it can be captured into a CUDA graph).
+int enqueue_packed(bcg_graph *g, const PackedRun &p, uint32_t S, cudaStream_t st);
+// Reads the control block after the stream has finished: error / overflow.
+int check_ctrl(bcg_graph *g, cudaStream_t st);
+// Rebuilds the work tiles with another shape (vcap vertices, ecap entries).
+int graph_retile(bcg_graph *g, uint32_t vcap, uint32_t ecap);
+
+}  // namespace bcg

@@ -747,15 +747,19 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
     const unsigned long long ring = 2ull * a.ntiles;
     const uint32_t total_warps = gridDim.x * kWarps;
 
+    const bool packed = a.xbeg != nullptr;
     for (uint32_t b = 0; b < a.nbatch; ++b) {
         if (threadIdx.x < S) {
-            sm.roots[threadIdx.x] = a.roots[(size_t)b * S + threadIdx.x];
-            sm.mult[threadIdx.x] = a.mult[(size_t)b * S + threadIdx.x];
+            sm.roots[threadIdx.x] = packed ? kNoRoot : a.roots[(size_t)b * S + threadIdx.x];
+            sm.mult[threadIdx.x] = packed ? 1.0 : a.mult[(size_t)b * S + threadIdx.x];
         }
         __syncthreads();
         // frontier / unvisited pair-edge counts of level 0 (same in every CTA)
         unsigned long long pf_cur = 0, pu_cur = 0;
-        {
+        if (packed) {
+            pf_cur = a.xpf[b];
+            pu_cur = a.xpu[b];
+        } else {
             unsigned int valid = 0;
 #pragma unroll
             for (int k = 0; k < S; ++k) {
@@ -809,6 +813,31 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
             for (int h = 0; h < R / 16; ++h) p[h] = make_uint4(w[4 * h], w[4 * h + 1], w[4 * h + 2], w[4 * h + 3]);
         }
         if (!grid_sync(c, nblk, wait_ns)) return;
+        if (packed) {
+            // seed the batch's roots once every row is reset: level 0 and
+            // sigma 1 in the root's slot, the slot counters, and the root's
+            // tile (all chunks for a hub) on level 0's list
+            const uint32_t key0 = tile_key(b, 0);
+            const uint32_t r0 = a.xbeg[b], r1 = a.xbeg[b + 1];
+            for (uint32_t i = r0 + blockIdx.x * blockDim.x + threadIdx.x; i < r1; i += gridDim.x * blockDim.x) {
+                const uint32_t r = a.xroots[i];
+                const int k = a.xslot[i];
+                unsigned char *row = row_of<S>(a, r);
+                *lvl_at(row, k) = 0;
+                *val_at<S>(row, k) = 1ull;
+                const uint2 ri = a.vinfo[r];
+                atomicAdd(&c->visited[k], 1ull);
+                atomicAdd(&c->wsum[k], 1ull + ri.y);
+                atomicAdd(&c->mc2[k], (unsigned long long)ri.x + 2ull * ri.y);
+                const uint32_t tf = a.tile_of[r];
+                const uint32_t t = tf & ~kHubFlag;
+                if (atomicExch(a.tmark + t, key0) == key0) continue;
+                const uint32_t nch = (tf & kHubFlag) ? a.tiles[t].nchunks : 1u;
+                const uint32_t base = atomicAdd(a.lcnt, nch);
+                for (uint32_t q = 0; q < nch; ++q) a.lists[base + q] = t + q;
+            }
+            if (!grid_sync(c, nblk, wait_ns)) return;
+        }
         trace(a, b, 0, 0, 0, 0);
 
         // ---- forward sweeps
@@ -847,7 +876,7 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
             __syncthreads();
             uint32_t walked;
             if (x.mode == kFwdPull) {
-                walked = uall ? a.ntiles : ulen;
+                walked = uall ? (packed ? a.xtiles[b] : a.ntiles) : ulen;
                 run_sweep<S>(a, sm, x, uall ? nullptr : a.ulist, ustart, walked, ring);
             } else {
                 walked = lc;
@@ -924,10 +953,10 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
         if (blockIdx.x == 0 && threadIdx.x < S) {
             const int k = threadIdx.x;
             const uint32_t r = sm.roots[k];
-            if (r != kNoRoot) {
+            if (r != kNoRoot || packed) {
                 const size_t idx = (size_t)b * S + k;
                 const unsigned long long W = vload64(&c->wsum[k]);
-                const uint32_t p = a.pend[idx];
+                const uint32_t p = packed ? 0u : a.pend[idx];
                 if (p && W >= 2) a.bc[r] += (double)p * (double)(W - 2);
                 a.rstat[idx].visited = vload64(&c->visited[k]);
                 a.rstat[idx].wsum = W;

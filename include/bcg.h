@@ -202,6 +202,41 @@ int bcg_run_weighted(bcg_graph *g, const uint32_t *roots, const double *mult,
 int bcg_set_batch_width(bcg_graph *g, uint32_t width);
 
 /* ---------------------------------------------------------------------------
+ * Batched form: exact all-sources BC of many independent graphs in one
+ * persistent launch.  The reference runs one graph per process (bc2d.c main);
+ * per graph the result is what bcg_run over all of its vertices gives.
+ * ------------------------------------------------------------------------ */
+
+typedef struct bcg_batch bcg_batch;   /* opaque: a set of graphs resident in HBM */
+
+/* Uploads ngraphs host CSR graphs (offsets[i][n[i] + 1], adj[i], undirected,
+ * lists as bcg_graph_create expects) as one disjoint union and builds the
+ * packed source schedule (every non-isolated vertex of every graph). */
+int bcg_batch_create(uint32_t ngraphs, const uint32_t *const *offsets,
+                     const uint32_t *const *adj, const uint32_t *n, bcg_batch **out);
+int bcg_batch_destroy(bcg_batch *b);
+
+/* Adds every graph's all-sources BC (ordered-pair sums) into its
+ * accumulator.  The first call captures the launch into a CUDA graph that
+ * later calls replay (bcg_batch_info reports whether the capture was made).
+ * stats: totals over all graphs; kernel_ms is the launch's device time. */
+int bcg_batch_run(bcg_batch *b, bcg_stats *stats);
+int bcg_batch_reset_bc(bcg_batch *b);
+/* Graph `graph`'s bc (n[graph] doubles, the creation order's numbering). */
+int bcg_batch_get_bc(bcg_batch *b, uint32_t graph, double *bc_host);
+
+/* Times the first sample_batches batches (0: 4) of the schedule for each
+ * batch width in {1, 3, 6} and each tile shape in {32x256, 32x128, 16x128,
+ * 16x64} (vertices x adjacency entries per tile), keeps the fastest per
+ * root and resets the accumulators.  Any output pointer may be NULL. */
+int bcg_batch_autotune(bcg_batch *b, uint32_t sample_batches, uint32_t *width,
+                       uint32_t *tile_vertices, uint32_t *tile_entries);
+/* Schedule length (packed batches), width, tile shape, and whether runs
+ * replay a captured CUDA graph (1) or launch directly (0). */
+int bcg_batch_info(bcg_batch *b, uint32_t *nbatch, uint32_t *width, uint32_t *tile_vertices,
+                   uint32_t *tile_entries, int *captured);
+
+/* ---------------------------------------------------------------------------
  * No-allocation entry point.  No counterpart in the reference: its
  * cuda_kernels.cu allocates all device state in initcuda (cuda_kernels.cu:
  * 1123-1198).  For callers that must not allocate device memory themselves
