@@ -190,6 +190,88 @@ def run_reference(args, rank, world):
     return 0
 
 
+def run_batched(args, rank, world):
+    """Batched form (all-sources exact BC of every graph) against the plain
+    per-graph loop (bcg_graph_create + bcg_run over all vertices + bcg_get_bc
+    + bcg_graph_destroy for each graph).  Graphs: the front of the seeded
+    2000-graph set (ck-bc_b200/workloads.py), optionally capped by scale.  One
+    GPU (replicas only: with N ranks every rank runs the same set)."""
+    import numpy as np
+    import torch
+
+    import bcg
+    import workloads
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    specs = [s for s in workloads.batched_specs()[:args.graphs] if workloads.spec_scale_ef(s)[0] <= args.max_scale]
+    t_gen = time.perf_counter()
+    graphs = [bcg.generate(s) for s in specs]
+    log(f"{len(graphs)} graphs generated in {time.perf_counter() - t_gen:.1f}s")
+    # plain loop (one warm-up graph first)
+    with bcg.Graph(*graphs[0]) as G:
+        G.run(np.arange(len(graphs[0][0]) - 1, dtype=np.uint32))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plain_edges, plain_kernel_ms = 0, 0.0
+    for offs, adj in graphs:
+        with bcg.Graph(offs, adj) as G:
+            st = G.run(np.arange(len(offs) - 1, dtype=np.uint32))
+            G.bc()
+        plain_edges += st.teps_edges
+        plain_kernel_ms += st.kernel_ms
+    plain_s = time.perf_counter() - t0
+    # batched: resident union, autotuned, captured launch replayed every step
+    t0 = time.perf_counter()
+    B = bcg.Batch(graphs)
+    create_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    tune = B.autotune()
+    tune_s = time.perf_counter() - t0
+    for _ in range(max(1, args.warmup)):
+        B.run()
+        B.reset()
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    kern, wall, edges = [], [], 0
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st = B.run()
+        for i in range(len(graphs)):
+            B.bc(i)
+        wall.append(time.perf_counter() - t0)
+        kern.append(st.kernel_ms)
+        edges = st.teps_edges
+        B.reset()
+    clk = clocks.stop()
+    info = B.info()
+    B.close()
+    assert edges == plain_edges, (edges, plain_edges)
+    k_s = sum(kern) / len(kern) / 1e3
+    w_s = sum(wall) / len(wall)
+    out = {"metric": "batched exact-BC TEPS (all sources of every graph)", "value": edges / k_s, "unit": "TEPS",
+           "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * k_s,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "impl": "bcg-batched",
+           "config": {"workload": "batched_2000_seed4_prefix", "graphs": len(graphs), "first": args.graphs,
+                      "max_scale": args.max_scale, "edges_per_step": edges, "width": info["width"],
+                      "tile": [info["tile_vertices"], info["tile_entries"]], "captured": info["captured"],
+                      "packed_batches": info["nbatch"]},
+           "graphs_per_s": len(graphs) / w_s,
+           "e2e": {"value": edges / w_s, "unit": "TEPS", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": int(8 * sum(len(o) - 1 for o, _ in graphs)),
+                   "path": "bcg_batch_run (resident union) + bcg_batch_get_bc per graph"},
+           "plain_loop": {"TEPS_wall": plain_edges / plain_s, "TEPS_kernel": plain_edges / (plain_kernel_ms / 1e3),
+                          "graphs_per_s": len(graphs) / plain_s, "wall_s": plain_s,
+                          "path": "per graph: bcg_graph_create + bcg_run(all) + bcg_get_bc + destroy"},
+           "speedup_vs_plain": {"kernel": (plain_kernel_ms / 1e3) / k_s, "wall": plain_s / w_s},
+           "setup_s": {"create": create_s, "autotune": tune_s, "choice": list(tune)},
+           "clocks": clk, "gpu_launches": 1}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -199,6 +281,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=0, help="e2e steps (default: min(steps, 3))")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sources", type=int, default=NSRC, help="sources per GPU (profiling runs use fewer)")
+    ap.add_argument("--form", default="plain", choices=["plain", "batched"],
+                    help="batched: the batched form on a prefix of the seeded 2000-graph set")
+    ap.add_argument("--graphs", type=int, default=120, help="batched form: graphs taken from the set's front")
+    ap.add_argument("--max-scale", type=int, default=16, help="batched form: keep graphs up to this scale")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -206,6 +292,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.form == "batched":
+        return run_batched(args, rank, world)
 
     import numpy as np
     import torch
