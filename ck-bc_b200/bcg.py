@@ -106,6 +106,13 @@ SIGNATURES = {
     "bcg_batch_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, _u32p, _u32p, _u32p]),
     "bcg_batch_info": (ctypes.c_int, [ctypes.c_void_p, _u32p, _u32p, _u32p, _u32p,
                                       ctypes.POINTER(ctypes.c_int)]),
+    "bcg_server_create": (ctypes.c_int, [ctypes.c_uint32, ctypes.POINTER(_u32p), ctypes.POINTER(_u32p), _u32p,
+                                         ctypes.c_uint64, ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p)]),
+    "bcg_server_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "bcg_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, _u32p, ctypes.c_uint64, _u64p]),
+    "bcg_server_step": (ctypes.c_int, [ctypes.c_void_p, _u64p, ctypes.c_uint32, _u32p]),
+    "bcg_server_result": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, _f64p]),
+    "bcg_server_info": (ctypes.c_int, [ctypes.c_void_p, _u64p, _u64p, _u32p, _u32p, _u64p]),
     "bcg_bc_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64,
                                       ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_int,
                                       ctypes.c_void_p]),
@@ -329,6 +336,74 @@ class Batch:
                                     ctypes.byref(cap)))
         return {"nbatch": nb.value, "width": w.value, "tile_vertices": tv.value, "tile_entries": te.value,
                 "captured": bool(cap.value)}
+
+
+class Server:
+    """Resident pool of graphs serving BC requests with continuous batching:
+    submit() queues, step() admits what fits and runs one wave, result()
+    returns a finished request's bc."""
+
+    def __init__(self, graphs, budget_bytes: int, wave_batches: int = 64):
+        self._keep = [(np.ascontiguousarray(o, dtype=np.uint32), np.ascontiguousarray(a, dtype=np.uint32))
+                      for o, a in graphs]
+        k = len(self._keep)
+        self.sizes = [len(o) - 1 for o, _ in self._keep]
+        offs = (_u32p * k)(*[_p32(o) for o, _ in self._keep])
+        adjs = (_u32p * k)(*[_p32(a) if len(a) else None for _, a in self._keep])
+        n = np.array(self.sizes, dtype=np.uint32)
+        h = ctypes.c_void_p()
+        _check(lib().bcg_server_create(k, offs, adjs, _p32(n), int(budget_bytes), wave_batches, ctypes.byref(h)))
+        self.h = h
+        self._graph_of = {}
+
+    def close(self):
+        if self.h:
+            lib().bcg_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, graph: int, sources=None) -> int:
+        """sources=None: exact BC (every vertex)."""
+        rid = ctypes.c_uint64()
+        if sources is None:
+            _check(lib().bcg_server_submit(self.h, graph, None, 0, ctypes.byref(rid)))
+        else:
+            s = np.ascontiguousarray(sources, dtype=np.uint32)
+            if len(s) == 0:
+                raise ValueError("a k-source request needs at least one source")
+            _check(lib().bcg_server_submit(self.h, graph, _p32(s), len(s), ctypes.byref(rid)))
+        self._graph_of[rid.value] = graph
+        return rid.value
+
+    def step(self, cap: int = 4096):
+        ids = (ctypes.c_uint64 * cap)()
+        nd = ctypes.c_uint32()
+        _check(lib().bcg_server_step(self.h, ids, cap, ctypes.byref(nd)))
+        return [ids[i] for i in range(nd.value)]
+
+    def result(self, rid: int) -> np.ndarray:
+        out = np.zeros(self.sizes[self._graph_of.pop(rid)], dtype=np.float64)
+        _check(lib().bcg_server_result(self.h, rid, out.ctypes.data_as(_f64p)))
+        return out
+
+    def info(self):
+        rb, ab, w = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        pend, run = ctypes.c_uint32(), ctypes.c_uint32()
+        _check(lib().bcg_server_info(self.h, ctypes.byref(rb), ctypes.byref(ab), ctypes.byref(pend),
+                                     ctypes.byref(run), ctypes.byref(w)))
+        return {"resident_bytes": rb.value, "admitted_bytes": ab.value, "pending": pend.value,
+                "running": run.value, "waves": w.value}
 
 
 def bc_noalloc(d_offsets: int, d_adj: int, n: int, nnz: int, d_sources: int, nsrc: int, d_bc: int,

@@ -35,7 +35,8 @@ struct bcg_batch {
     std::vector<uint32_t> hdeg;      // union degrees
     uint32_t width = 3;
     // device schedule of the current width and tile shape
-    uint32_t *d_xbeg = nullptr, *d_xroots = nullptr, *d_xtiles = nullptr;
+    uint32_t *d_xbeg = nullptr, *d_xroots = nullptr, *d_xtiles = nullptr, *d_xrbeg = nullptr;
+    uint2 *d_xrange = nullptr;
     unsigned char *d_xslot = nullptr;
     unsigned long long *d_xpf = nullptr, *d_xpu = nullptr;
     RootStat *d_rstat = nullptr;
@@ -61,8 +62,9 @@ namespace {
 
 void free_schedule(bcg_batch *b) {
     cudaFree(b->d_xbeg); cudaFree(b->d_xroots); cudaFree(b->d_xtiles); cudaFree(b->d_xslot);
-    cudaFree(b->d_xpf); cudaFree(b->d_xpu); cudaFree(b->d_rstat);
-    b->d_xbeg = b->d_xroots = b->d_xtiles = nullptr;
+    cudaFree(b->d_xpf); cudaFree(b->d_xpu); cudaFree(b->d_rstat); cudaFree(b->d_xrbeg); cudaFree(b->d_xrange);
+    b->d_xbeg = b->d_xroots = b->d_xtiles = b->d_xrbeg = nullptr;
+    b->d_xrange = nullptr;
     b->d_xslot = nullptr;
     b->d_xpf = b->d_xpu = nullptr;
     b->d_rstat = nullptr;
@@ -143,6 +145,14 @@ int build_schedule(bcg_batch *b) {
     CKB(cudaMemcpy(b->d_xtiles, xtiles.data(), nb * sizeof(uint32_t), cudaMemcpyHostToDevice));
     CKB(cudaMemcpy(b->d_xpf, xpf.data(), nb * sizeof(unsigned long long), cudaMemcpyHostToDevice));
     CKB(cudaMemcpy(b->d_xpu, xpu.data(), nb * sizeof(unsigned long long), cudaMemcpyHostToDevice));
+    // one tile range per batch: the active prefix [0, xtiles[i])
+    std::vector<uint32_t> xrbeg(nb + 1);
+    std::iota(xrbeg.begin(), xrbeg.end(), 0u);
+    std::vector<uint2> xrange(nb, make_uint2(0u, 0u));
+    CKB(cudaMalloc(&b->d_xrbeg, (nb + 1) * sizeof(uint32_t)));
+    CKB(cudaMalloc(&b->d_xrange, nb * sizeof(uint2)));
+    CKB(cudaMemcpy(b->d_xrbeg, xrbeg.data(), (nb + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    CKB(cudaMemcpy(b->d_xrange, xrange.data(), nb * sizeof(uint2), cudaMemcpyHostToDevice));
     return ensure_state(g, S);
 }
 
@@ -154,6 +164,8 @@ PackedRun packed_prefix(const bcg_batch *b, uint32_t nbatch) {
     p.xpf = b->d_xpf;
     p.xpu = b->d_xpu;
     p.xtiles = b->d_xtiles;
+    p.xrbeg = b->d_xrbeg;
+    p.xrange = b->d_xrange;
     p.nbatch = nbatch;
     p.rstat = b->d_rstat;
     return p;
@@ -173,12 +185,11 @@ int timed_run(bcg_batch *b, uint32_t nbatch, float *ms) {
 
 }  // namespace
 
-extern "C" {
+namespace bcg {
 
-int bcg_batch_create(uint32_t ngraphs, const uint32_t *const *offsets, const uint32_t *const *adj,
-                     const uint32_t *n, bcg_batch **out) {
-    clear_error();
-    if (!out) return set_error(BCG_ERR_ARG, "null output handle");
+int make_union(uint32_t ngraphs, const uint32_t *const *offsets, const uint32_t *const *adj, const uint32_t *n,
+               bool by_active, std::vector<uint32_t> &order, std::vector<uint32_t> &base,
+               std::vector<uint32_t> &hdeg, bcg_graph **out) {
     *out = nullptr;
     if (ngraphs == 0 || !offsets || !adj || !n) return set_error(BCG_ERR_ARG, "no graphs or null arrays");
     uint64_t N = 0, NNZ = 0;
@@ -190,45 +201,56 @@ int bcg_batch_create(uint32_t ngraphs, const uint32_t *const *offsets, const uin
     }
     if (N > 0xFFFFFFFEull || NNZ > 0xFFFFFFFFull)
         return set_error(BCG_ERR_RANGE, "union of %u graphs exceeds 32-bit ids/offsets", ngraphs);
-    bcg_batch *b = new bcg_batch();
-    b->ngraphs = ngraphs;
-    b->base.resize(ngraphs);
-    b->gn.assign(n, n + ngraphs);
-    // union order: most non-isolated vertices first
-    std::vector<uint32_t> act(ngraphs, 0);
-    for (uint32_t i = 0; i < ngraphs; ++i)
-        for (uint32_t v = 0; v < n[i]; ++v) act[i] += (offsets[i][v + 1] > offsets[i][v]);
-    b->order.resize(ngraphs);
-    std::iota(b->order.begin(), b->order.end(), 0u);
-    std::stable_sort(b->order.begin(), b->order.end(), [&](uint32_t x, uint32_t y) { return act[x] > act[y]; });
+    order.resize(ngraphs);
+    std::iota(order.begin(), order.end(), 0u);
+    if (by_active) {
+        // most non-isolated vertices first
+        std::vector<uint32_t> act(ngraphs, 0);
+        for (uint32_t i = 0; i < ngraphs; ++i)
+            for (uint32_t v = 0; v < n[i]; ++v) act[i] += (offsets[i][v + 1] > offsets[i][v]);
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return act[x] > act[y]; });
+    }
+    base.assign(ngraphs, 0);
     std::vector<uint32_t> uoffs(N + 1), uadj(NNZ);
-    b->hdeg.resize(N);
+    hdeg.resize(N);
     uint64_t vpos = 0, epos = 0;
     for (uint32_t p = 0; p < ngraphs; ++p) {
-        const uint32_t gi = b->order[p];
+        const uint32_t gi = order[p];
         const uint32_t vb = (uint32_t)vpos;
-        b->base[gi] = vb;
+        base[gi] = vb;
         const uint32_t *o = offsets[gi];
         for (uint32_t v = 0; v < n[gi]; ++v) {
             uoffs[vpos] = (uint32_t)epos;
-            b->hdeg[vpos] = o[v + 1] - o[v];
+            hdeg[vpos] = o[v + 1] - o[v];
             for (uint32_t e = o[v]; e < o[v + 1]; ++e) {
                 const uint32_t w = adj[gi][e];
-                if (w >= n[gi]) {
-                    delete b;
-                    return set_error(BCG_ERR_ARG, "graph %u: adj[%u] = %u >= n=%u", gi, e, w, n[gi]);
-                }
+                if (w >= n[gi]) return set_error(BCG_ERR_ARG, "graph %u: adj[%u] = %u >= n=%u", gi, e, w, n[gi]);
                 uadj[epos++] = vb + w;
             }
             ++vpos;
         }
     }
     uoffs[N] = (uint32_t)epos;
-    int rc = bcg_graph_create(uoffs.data(), uadj.data(), (uint32_t)N, NNZ, 0, &b->g);
+    return bcg_graph_create(uoffs.data(), uadj.data(), (uint32_t)N, NNZ, 0, out);
+}
+
+}  // namespace bcg
+
+extern "C" {
+
+int bcg_batch_create(uint32_t ngraphs, const uint32_t *const *offsets, const uint32_t *const *adj,
+                     const uint32_t *n, bcg_batch **out) {
+    clear_error();
+    if (!out) return set_error(BCG_ERR_ARG, "null output handle");
+    *out = nullptr;
+    bcg_batch *b = new bcg_batch();
+    int rc = make_union(ngraphs, offsets, adj, n, true, b->order, b->base, b->hdeg, &b->g);
     if (rc) {
         delete b;
         return rc;
     }
+    b->ngraphs = ngraphs;
+    b->gn.assign(n, n + ngraphs);
     auto fail = [&](int code) {
         bcg_batch_destroy(b);
         return code;

@@ -124,15 +124,20 @@ __global__ void k_levels_out(uint32_t n, const unsigned char *__restrict__ rows,
 // Runs of at most vcap consecutive vertices with at most ecap adjacency
 // entries; a vertex with more than ecap entries is split into ecap-entry
 // chunks (vcap <= 32, ecap <= 256: the sweep kernel's lane and run limits).
-// tile_of[v] = index of v's tile (of its first chunk, with kHubFlag, when v
-// is split).
-static void build_tiles(const uint32_t *offs, uint32_t n, uint32_t vcap, uint32_t ecap, std::vector<Tile> &tiles,
-                        uint32_t &nhub, std::vector<uint32_t> &tile_of) {
+// A tile never spans a vertex listed in `breaks` (sorted) and the vertex
+// before it.  tile_of[v] = index of v's tile (of its first chunk, with
+// kHubFlag, when v is split).
+static void build_tiles(const uint32_t *offs, uint32_t n, uint32_t vcap, uint32_t ecap,
+                        const std::vector<uint32_t> &breaks, std::vector<Tile> &tiles, uint32_t &nhub,
+                        std::vector<uint32_t> &tile_of) {
     tiles.clear();
     tile_of.assign(n, 0);
     nhub = 0;
     uint32_t v = 0;
+    size_t nb = 0;  // next break point
     while (v < n) {
+        while (nb < breaks.size() && breaks[nb] <= v) ++nb;
+        const uint32_t stop = nb < breaks.size() ? breaks[nb] : n;
         const uint32_t dv = offs[v + 1] - offs[v];
         if (dv > ecap) {
             const uint32_t nch = (dv + ecap - 1) / ecap;
@@ -152,7 +157,7 @@ static void build_tiles(const uint32_t *offs, uint32_t n, uint32_t vcap, uint32_
         }
         const uint32_t start = v;
         uint32_t sum = 0;
-        while (v < n && v - start < vcap) {
+        while (v < stop && v - start < vcap) {
             const uint32_t d = offs[v + 1] - offs[v];
             if (d > ecap || sum + d > ecap) break;
             sum += d;
@@ -243,7 +248,7 @@ static int setup_tiles(bcg_graph *g, const uint32_t *h_offs) {
     const uint32_t n = g->n;
     std::vector<Tile> tiles;
     std::vector<uint32_t> tile_of;
-    build_tiles(h_offs, n, g->tile_vcap, g->tile_ecap, tiles, g->nhub, tile_of);
+    build_tiles(h_offs, n, g->tile_vcap, g->tile_ecap, g->tile_breaks, tiles, g->nhub, tile_of);
     g->ntiles = (uint32_t)tiles.size();
     CK(cudaMalloc(&g->d_tiles, std::max<size_t>(1, tiles.size()) * sizeof(Tile)));
     if (!tiles.empty())
@@ -298,11 +303,11 @@ static int create_common(bcg_graph *g, const uint32_t *h_offs) {
     return BCG_OK;
 }
 
-int graph_retile(bcg_graph *g, uint32_t vcap, uint32_t ecap) {
+int graph_retile(bcg_graph *g, uint32_t vcap, uint32_t ecap, bool force) {
     if (vcap < 1 || vcap > (uint32_t)kTileVerts || ecap < 1 || ecap > (uint32_t)kTileEdges)
         return set_error(BCG_ERR_ARG, "tile shape %ux%u outside 1..%d vertices, 1..%d entries", vcap, ecap,
                          kTileVerts, kTileEdges);
-    if (vcap == g->tile_vcap && ecap == g->tile_ecap) return BCG_OK;
+    if (!force && vcap == g->tile_vcap && ecap == g->tile_ecap) return BCG_OK;
     std::vector<uint32_t> h_offs((size_t)g->n + 1);
     CK(cudaMemcpy(h_offs.data(), g->d_offs, h_offs.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
     cudaFree(g->d_tiles); cudaFree(g->d_tile_of); cudaFree(g->d_tmark); cudaFree(g->d_ulist);
@@ -545,6 +550,8 @@ int enqueue_packed(bcg_graph *g, const PackedRun &p, uint32_t S, cudaStream_t st
     a.xpf = p.xpf;
     a.xpu = p.xpu;
     a.xtiles = p.xtiles;
+    a.xrbeg = p.xrbeg;
+    a.xrange = p.xrange;
     int grid = 0;
     return launch_sweep((int)S, a, st, &grid);
 }

@@ -134,14 +134,17 @@ struct BatchArgs {
     // weight 1 and no pendant sources; the per-slot counters add up over its
     // roots.  xpu[b] = sum over the batch's roots of the adjacency entries of
     // their components minus their own degrees (level 0's unvisited
-    // pair-edges); the first xtiles[b] tiles hold every vertex of those
-    // components (the first pull of the batch walks only them).
+    // pair-edges).  The tiles of those components are the ranges
+    // xrange[xrbeg[b] .. xrbeg[b+1]) ({first tile, tiles before this range});
+    // xtiles[b] is their total: the first pull of the batch walks only them.
     const uint32_t *xbeg;
     const uint32_t *xroots;
     const unsigned char *xslot;
     const unsigned long long *xpf;   // per batch: sum of the roots' degrees
     const unsigned long long *xpu;
     const uint32_t *xtiles;
+    const uint32_t *xrbeg;
+    const uint2 *xrange;
 };
 
 }  // namespace bcg

@@ -43,6 +43,7 @@ struct bcg_graph {
     std::vector<uint32_t> h_anchor;  // empty when not pruned
     uint32_t forced_width = 0;
     uint32_t tile_vcap = kTileVerts, tile_ecap = kTileEdges;  // tile shape (autotuned by batches)
+    std::vector<uint32_t> tile_breaks;  // sorted vertices where a new tile must start
     float ratio = 0.2f;
     unsigned long long wait_ns = kDefaultWaitNs;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -57,7 +58,8 @@ struct PackedRun {
     const uint32_t *xbeg, *xroots;
     const unsigned char *xslot;
     const unsigned long long *xpf, *xpu;
-    const uint32_t *xtiles;
+    const uint32_t *xtiles, *xrbeg;
+    const uint2 *xrange;
     uint32_t nbatch;
     RootStat *rstat;  // nbatch * S per-slot totals
 };
@@ -70,6 +72,12 @@ int enqueue_packed(bcg_graph *g, const PackedRun &p, uint32_t S, cudaStream_t st
 // Reads the control block after the stream has finished: error / overflow.
 int check_ctrl(bcg_graph *g, cudaStream_t st);
 // Rebuilds the work tiles with another shape (vcap vertices, ecap entries).
-int graph_retile(bcg_graph *g, uint32_t vcap, uint32_t ecap);
+int graph_retile(bcg_graph *g, uint32_t vcap, uint32_t ecap, bool force = false);
+// Uploads ngraphs host CSR graphs as one disjoint union (graph order[p] at
+// union position p, its vertex v at base[order[p]] + v; with by_active the
+// graphs with most non-isolated vertices come first).  hdeg: union degrees.
+int make_union(uint32_t ngraphs, const uint32_t *const *offsets, const uint32_t *const *adj, const uint32_t *n,
+               bool by_active, std::vector<uint32_t> &order, std::vector<uint32_t> &base,
+               std::vector<uint32_t> &hdeg, bcg_graph **out);
 
 }  // namespace bcg

@@ -670,9 +670,12 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
 // of the list), and its warps take them one at a time from a shared counter
 // (sm.next, zeroed before the sweep), so a warp that drew cheap tiles keeps
 // working instead of waiting at the sweep's barrier.
+// With no list and a range table, item i is tile ranges[r].x + (i - ranges[r].y)
+// for the last range r with ranges[r].y <= i (nranges ranges, increasing .y).
 template <int S>
 __device__ void run_sweep(const BatchArgs &a, Smem<S> &sm, const SweepCtx &x, const uint32_t *list,
-                          unsigned long long start, uint32_t nwork, unsigned long long ring) {
+                          unsigned long long start, uint32_t nwork, unsigned long long ring,
+                          const uint2 *ranges = nullptr, uint32_t nranges = 0) {
     const unsigned wid = threadIdx.x >> 5;
     WarpSmem<S> &ws = sm.w[wid];
     if ((threadIdx.x & 31) == 0) {
@@ -685,7 +688,15 @@ __device__ void run_sweep(const BatchArgs &a, Smem<S> &sm, const SweepCtx &x, co
     const unsigned long long nitems = (unsigned long long)nwork * x.split;
     auto item_tile = [&](unsigned long long it) -> uint32_t {
         const uint32_t i = (uint32_t)(it / x.split);
-        return list ? list[(start + i) % ring] : i;
+        if (list) return list[(start + i) % ring];
+        if (!ranges) return i;
+        uint32_t lo = 0, hi = nranges;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (ranges[mid].y <= i) lo = mid; else hi = mid;
+        }
+        const uint2 r = ranges[lo];
+        return r.x + (i - r.y);
     };
     const unsigned long long G = gridDim.x;
     auto grab = [&]() -> unsigned long long {
@@ -877,7 +888,9 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
             uint32_t walked;
             if (x.mode == kFwdPull) {
                 walked = uall ? (packed ? a.xtiles[b] : a.ntiles) : ulen;
-                run_sweep<S>(a, sm, x, uall ? nullptr : a.ulist, ustart, walked, ring);
+                const bool ranged = uall && packed;
+                run_sweep<S>(a, sm, x, uall ? nullptr : a.ulist, ustart, walked, ring,
+                             ranged ? a.xrange + a.xrbeg[b] : nullptr, ranged ? a.xrbeg[b + 1] - a.xrbeg[b] : 0u);
             } else {
                 walked = lc;
                 run_sweep<S>(a, sm, x, a.lists + lb, 0, lc, 0xFFFFFFFFull);

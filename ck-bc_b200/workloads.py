@@ -39,3 +39,36 @@ def batched_specs(count: int = 2000, seed: int = 4, smin: float = 8.0, smax: flo
 def spec_scale_ef(spec: str) -> tuple[int, int]:
     kv = dict(p.split("=") for p in spec.split(":", 1)[1].split(","))
     return int(kv["scale"]), int(kv["ef"])
+
+
+# Serving form: a pool of 64 resident R-MAT graphs (scale uniform in 10..22,
+# edge factor 16, seed 5) and a Poisson stream of BC requests (seed 5): each
+# request names a graph uniformly at random and is exact BC (every vertex)
+# or k-source BC with k log-uniform in [64, 1024] (rounded, at most the
+# graph's vertex count) and the sources drawn uniformly without replacement.
+def serving_pool(count: int = 64, seed: int = 5, smin: int = 10, smax: int = 22, ef: int = 16) -> list[str]:
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for _ in range(count):
+        scale = int(rng.integers(smin, smax + 1))
+        out.append(f"rmat:scale={scale},ef={ef},{RMAT_ABC},seed={int(rng.integers(1, 2**62))}")
+    return out
+
+
+def serving_stream(sizes: list[int], count: int = 20000, seed: int = 5, rate: float = 100.0,
+                   kmin: int = 64, kmax: int = 1024):
+    """-> list of (arrival_s, graph, sources or None for exact); `rate` is the
+    Poisson arrival rate in requests per second."""
+    rng = np.random.Generator(np.random.PCG64(seed + 1000003))
+    t = 0.0
+    reqs = []
+    for _ in range(count):
+        t += float(rng.exponential(1.0 / rate))
+        g = int(rng.integers(0, len(sizes)))
+        if rng.random() < 0.5:
+            reqs.append((t, g, None))
+        else:
+            k = int(round(math.exp(rng.uniform(math.log(kmin), math.log(kmax)))))
+            k = min(k, sizes[g])
+            reqs.append((t, g, np.sort(rng.choice(sizes[g], size=k, replace=False)).astype(np.uint32)))
+    return reqs

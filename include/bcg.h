@@ -237,6 +237,42 @@ int bcg_batch_info(bcg_batch *b, uint32_t *nbatch, uint32_t *width, uint32_t *ti
                    uint32_t *tile_entries, int *captured);
 
 /* ---------------------------------------------------------------------------
+ * Serving form: BC requests against a pool of resident graphs, admitted
+ * under an HBM budget and run with continuous batching.  The reference
+ * answers one query per process run (bc2d.c main); per request the result is
+ * what bcg_run over the request's sources gives on that graph.
+ * ------------------------------------------------------------------------ */
+
+typedef struct bcg_server bcg_server;  /* opaque: a resident pool and its requests */
+
+/* Uploads the pool (as bcg_batch_create) and sizes the wave schedule:
+ * wave_batches = batches of S sources each graph may advance per wave
+ * (1..65535).  Fails with BCG_ERR_OOM when the pool alone exceeds
+ * hbm_budget_bytes. */
+int bcg_server_create(uint32_t ngraphs, const uint32_t *const *offsets,
+                      const uint32_t *const *adj, const uint32_t *n,
+                      uint64_t hbm_budget_bytes, uint32_t wave_batches, bcg_server **out);
+int bcg_server_destroy(bcg_server *s);
+/* Queues a request: BC of graph `graph` over sources[nsrc] (nsrc == 0: every
+ * vertex of the graph, i.e. exact BC).  Sources of degree 0 are skipped, as
+ * in bcg_run.  Its result buffer (8 bytes per vertex of the graph) is
+ * allocated when the request is admitted, first come first served, while the
+ * pool plus admitted buffers fit the budget. */
+int bcg_server_submit(bcg_server *s, uint32_t graph, const uint32_t *sources, uint64_t nsrc,
+                      uint64_t *id);
+/* Admits what fits, runs one wave (every graph with an admitted request
+ * advances its oldest one by up to wave_batches * S sources, all in one
+ * packed launch), and reports up to cap finished request ids. */
+int bcg_server_step(bcg_server *s, uint64_t *done_ids, uint32_t cap, uint32_t *ndone);
+/* Copies a finished request's bc (ordered-pair sums, n doubles of its
+ * graph) and releases its buffer and the request. */
+int bcg_server_result(bcg_server *s, uint64_t id, double *bc_host);
+/* Pool bytes, admitted buffer bytes, requests waiting for admission,
+ * admitted unfinished requests, waves run so far.  Outputs may be NULL. */
+int bcg_server_info(bcg_server *s, uint64_t *resident_bytes, uint64_t *admitted_bytes,
+                    uint32_t *pending, uint32_t *running, uint64_t *waves);
+
+/* ---------------------------------------------------------------------------
  * No-allocation entry point.  No counterpart in the reference: its
  * cuda_kernels.cu allocates all device state in initcuda (cuda_kernels.cu:
  * 1123-1198).  For callers that must not allocate device memory themselves
