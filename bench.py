@@ -272,6 +272,134 @@ def run_batched(args, rank, world):
     return 0
 
 
+def run_serve(args, rank, world):
+    """Serving form against the plain per-request loop on the front of the
+    seeded request stream (ck-bc_b200/workloads.py: pool of 64 R-MAT graphs,
+    Poisson arrivals, exact or k-source requests).  Exact requests on graphs
+    above --exact-max-scale are left out of both arms and counted.  Plain
+    loop: the pool resident as one bcg_graph per graph, each request in
+    arrival order as bcg_reset_bc + bcg_run(sources) + bcg_get_bc; its Poisson
+    latencies replay the measured service times through a FIFO queue.
+    Served: bcg_server (HBM budget 150 GB); throughput with every request
+    queued at once, latency from a real-time replay of Poisson arrivals at
+    half the served throughput.  One GPU (replicas only)."""
+    import numpy as np
+    import torch
+
+    import bcg
+    import workloads
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    specs = workloads.serving_pool()
+    t_gen = time.perf_counter()
+    pool = [bcg.generate(s) for s in specs]
+    sizes = [len(o) - 1 for o, _ in pool]
+    log(f"pool of {len(pool)} graphs generated in {time.perf_counter() - t_gen:.1f}s, "
+        f"{sum(sizes)} vertices, {sum(len(a) for _, a in pool)} entries")
+    scale = [workloads.spec_scale_ef(s)[0] for s in specs]
+    stream = workloads.serving_stream(sizes)
+    reqs, left_out = [], 0
+    for t, g, src in stream:
+        if len(reqs) >= args.requests:
+            break
+        if src is None and scale[g] > args.exact_max_scale:
+            left_out += 1
+            continue
+        reqs.append((g, src))
+    n_exact = sum(1 for _, s in reqs if s is None)
+
+    # ---- plain loop
+    handles = [bcg.Graph(o, a) for o, a in pool]
+    with bcg.Graph(*pool[0]) as G:
+        G.run(np.arange(min(64, sizes[0]), dtype=np.uint32))
+    torch.cuda.synchronize()
+    service = []
+    plain_res = []
+    t0 = time.perf_counter()
+    for g, src in reqs:
+        ts = time.perf_counter()
+        H = handles[g]
+        H.reset()
+        H.run(np.arange(sizes[g], dtype=np.uint32) if src is None else src)
+        plain_res.append(H.bc())
+        service.append(time.perf_counter() - ts)
+    plain_s = time.perf_counter() - t0
+    for H in handles:
+        H.close()
+    plain_rps = len(reqs) / plain_s
+
+    budget = 150 * 10**9
+
+    def serve(arrivals):
+        done_at = {}
+        S = bcg.Server(pool, budget, args.wave_batches)
+        ids = [None] * len(reqs)
+        results = {}
+        t_start = time.perf_counter()
+        nxt = 0
+        while len(done_at) < len(reqs):
+            now = time.perf_counter() - t_start
+            while nxt < len(reqs) and arrivals[nxt] <= now:
+                g, src = reqs[nxt]
+                ids[nxt] = S.submit(g, src)
+                nxt += 1
+            if nxt == len(done_at) and nxt < len(reqs):
+                time.sleep(max(0.0, min(0.001, arrivals[nxt] - now)))
+                continue
+            for rid in S.step():
+                done_at[rid] = time.perf_counter() - t_start
+                results[rid] = S.result(rid)
+        info = S.info()
+        S.close()
+        lat = [done_at[ids[i]] - arrivals[i] for i in range(len(reqs))]
+        span = max(done_at.values())
+        return lat, span, info, [results[ids[i]] for i in range(len(reqs))]
+
+    lat_sat, span_sat, info_sat, served_res = serve([0.0] * len(reqs))
+    served_rps = len(reqs) / span_sat
+    # results agree with the plain loop
+    worst = 0.0
+    for a, b in zip(served_res, plain_res):
+        worst = max(worst, float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1.0))) if len(a) else 0.0)
+    rate = 0.5 * served_rps
+    arr = np.cumsum(np.random.Generator(np.random.PCG64(5)).exponential(1.0 / rate, size=len(reqs)))
+    arr = [float(x) for x in arr]
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    lat, span, info, _ = serve(arr)
+    clk = clocks.stop()
+    # the plain loop at the same arrivals: FIFO replay of its service times
+    free, plat = 0.0, []
+    for a, sv in zip(arr, service):
+        start = max(a, free)
+        free = start + sv
+        plat.append(free - a)
+
+    def pct(x, q):
+        return float(np.percentile(np.asarray(x), q))
+
+    out = {"metric": "served BC requests/s (exact and k-source, seeded Poisson stream)", "value": served_rps,
+           "unit": "req/s", "n_gpus": world, "steps": 1, "warmup": 0, "ms_per_step": 1e3 * span_sat,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "impl": "bcg-served",
+           "config": {"workload": "serving_pool64_stream_seed5_prefix", "requests": len(reqs), "exact": n_exact,
+                      "k_source": len(reqs) - n_exact, "exact_left_out_above_scale": args.exact_max_scale,
+                      "exact_left_out": left_out, "wave_batches": args.wave_batches, "hbm_budget_bytes": budget,
+                      "resident_bytes": info["resident_bytes"], "pool_vertices": sum(sizes)},
+           "plain_loop": {"req_per_s": plain_rps, "wall_s": plain_s,
+                          "p50_s": pct(plat, 50), "p99_s": pct(plat, 99),
+                          "path": "resident bcg_graph per graph; per request bcg_reset_bc + bcg_run + bcg_get_bc"},
+           "speedup_vs_plain": served_rps / plain_rps,
+           "latency": {"arrival_rate_per_s": rate, "p50_s": pct(lat, 50), "p99_s": pct(lat, 99),
+                       "makespan_s": span, "waves": info["waves"]},
+           "saturated": {"makespan_s": span_sat, "p50_s": pct(lat_sat, 50), "p99_s": pct(lat_sat, 99),
+                         "waves": info_sat["waves"]},
+           "max_rel_diff_vs_plain": worst, "clocks": clk, "gpu_launches": info_sat["waves"]}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -281,10 +409,14 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=0, help="e2e steps (default: min(steps, 3))")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sources", type=int, default=NSRC, help="sources per GPU (profiling runs use fewer)")
-    ap.add_argument("--form", default="plain", choices=["plain", "batched"],
+    ap.add_argument("--form", default="plain", choices=["plain", "batched", "serve"],
                     help="batched: the batched form on a prefix of the seeded 2000-graph set")
     ap.add_argument("--graphs", type=int, default=120, help="batched form: graphs taken from the set's front")
     ap.add_argument("--max-scale", type=int, default=16, help="batched form: keep graphs up to this scale")
+    ap.add_argument("--requests", type=int, default=200, help="serving form: requests taken from the stream's front")
+    ap.add_argument("--exact-max-scale", type=int, default=16,
+                    help="serving form: exact requests on larger graphs are left out (hours each)")
+    ap.add_argument("--wave-batches", type=int, default=64, help="serving form: batches per graph per wave")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -294,6 +426,8 @@ def main():
         return run_reference(args, rank, world)
     if args.form == "batched":
         return run_batched(args, rank, world)
+    if args.form == "serve":
+        return run_serve(args, rank, world)
 
     import numpy as np
     import torch

@@ -10,8 +10,8 @@
 // (i*S + k)-th non-isolated vertex of every graph that has that many, so one
 // batch advances every active graph at once and the sweeps of small graphs
 // share the grid barriers of the large ones.  Graphs still active in batch i
-// are a prefix of the union, so the first pull of the batch walks only the
-// tiles of that prefix.  The whole schedule runs in one cooperative launch,
+// are a prefix of the union and tiles never cross a graph boundary, so a
+// batch resets and first pulls only the rows and tiles of that prefix.  The whole schedule runs in one cooperative launch,
 // captured once into a CUDA graph and replayed by every bcg_batch_run.
 //
 // The autotuner times a prefix of the schedule for each candidate batch width
@@ -117,14 +117,9 @@ int build_schedule(bcg_batch *b) {
             }
         }
         xbeg[i + 1] = (uint32_t)xroots.size();
-        // tiles of the active prefix: up to and including the tile of the first
-        // vertex past it (a tile may straddle two graphs)
-        if (last_active >= G) {
-            xtiles[i] = g->ntiles;
-        } else {
-            const uint32_t v_end = b->base[b->order[last_active]];
-            xtiles[i] = std::min(g->ntiles, (tile_of[v_end] & ~kHubFlag) + 1);
-        }
+        // tiles of the active prefix: every tile before the first inactive
+        // graph's (tiles never cross a graph boundary)
+        xtiles[i] = (last_active >= G) ? g->ntiles : (tile_of[b->base[b->order[last_active]]] & ~kHubFlag);
     }
     b->nbatch = nb;
     b->nroots = xroots.size();
@@ -251,6 +246,16 @@ int bcg_batch_create(uint32_t ngraphs, const uint32_t *const *offsets, const uin
     }
     b->ngraphs = ngraphs;
     b->gn.assign(n, n + ngraphs);
+    // tiles never cross a graph boundary: a batch then reaches exactly the
+    // rows of its active graphs, and only those are reset and walked
+    std::vector<uint32_t> breaks(b->base);
+    std::sort(breaks.begin(), breaks.end());
+    b->g->tile_breaks = breaks;
+    rc = graph_retile(b->g, b->g->tile_vcap, b->g->tile_ecap, true);
+    if (rc) {
+        bcg_batch_destroy(b);
+        return rc;
+    }
     auto fail = [&](int code) {
         bcg_batch_destroy(b);
         return code;

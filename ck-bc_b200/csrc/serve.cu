@@ -13,15 +13,15 @@
 // advances its first request by a chunk of up to wave_batches * S sources, all
 // of them packed into one persistent launch (component-packed batches: a
 // graph's sources fill the S slots of successive batches, graphs share the
-// batches).  The first pull of a batch walks only the tile ranges of the
+// batches; S is 6 while the active graphs' 64-byte state rows fit 64 MB, as
+// in bcg_run, else 3).  The first pull of a batch walks only the tile ranges of the
 // graphs active in it.  After the launch a drain kernel adds each active
 // graph's slice of the union's bc into its request's buffer and clears the
 // slice.  A request that arrives while a wave runs joins the next one, so the
 // GPU always works on every admitted request at once, and large requests do
-// not hold small ones back for longer than one wave.  A request's chunks and
-// batches do not depend on the other requests, so its result is the same
-// alone and in a mix (up to the order of the floating-point adds of hub
-// chunks).
+// not hold small ones back for longer than one wave.  Every source of a
+// request adds the same dependencies alone or in a mix; only the grouping of
+// those floating-point sums into waves may differ with the wave width.
 #include <algorithm>
 #include <deque>
 #include <unordered_map>
@@ -72,7 +72,7 @@ struct bcg_server {
     std::vector<uint2> grange;    // per caller graph: its tiles [x, y)
     std::vector<uint64_t> gnnz;
     uint64_t budget = 0, resident = 0, admitted = 0;
-    uint32_t width = 3, wave_batches = 64;
+    uint32_t width = 6, wave_batches = 64;  // width: the widest a wave may use
     std::unordered_map<uint64_t, Req> reqs;
     uint64_t next_id = 1;
     std::deque<uint64_t> pending;
@@ -243,10 +243,12 @@ int bcg_server_step(bcg_server *s, uint64_t *done_ids, uint32_t cap, uint32_t *n
     *ndone = 0;
     int rc = admit(s);
     if (rc) return rc;
-    const uint32_t S = s->width, G = s->ngraphs, W = s->wave_batches;
-    // the chunk each active graph runs in this wave
+    const uint32_t G = s->ngraphs, W = s->wave_batches;
+    // the graphs active in this wave; the wave's width follows bcg_run's rule:
+    // 6 sources per batch while the active graphs' 64-byte state rows fit
+    // 64 MB (they then stay in L2), else 3
     std::vector<uint32_t> act;  // caller graph ids
-    std::vector<size_t> c0, c1;
+    uint64_t act_n = 0;
     for (uint32_t gi = 0; gi < G; ++gi) {
         auto &q = s->queue[gi];
         while (!q.empty() && s->reqs[q.front()].next >= s->reqs[q.front()].src.size()) {
@@ -255,8 +257,13 @@ int bcg_server_step(bcg_server *s, uint64_t *done_ids, uint32_t cap, uint32_t *n
             q.pop_front();
         }
         if (q.empty()) continue;
-        const Req &r = s->reqs[q.front()];
         act.push_back(gi);
+        act_n += s->gn[gi];
+    }
+    const uint32_t S = (act_n * (uint64_t)row_bytes(6) <= (64ull << 20)) ? 6u : 3u;
+    std::vector<size_t> c0, c1;  // the chunk each active graph runs in this wave
+    for (uint32_t gi : act) {
+        const Req &r = s->reqs[s->queue[gi].front()];
         c0.push_back(r.next);
         c1.push_back(std::min(r.src.size(), r.next + (size_t)W * S));
     }

@@ -804,24 +804,39 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
             }
             a.lcnt[0] = n0;
         }
-        // reset every row; roots at level 0 with sigma 1
-        for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < a.n;
-             v += (size_t)gridDim.x * blockDim.x) {
-            constexpr int VW = RowGeom<S>::kValWord;
-            uint32_t w[R / 4];
+        // reset the rows the batch can reach (every row; in a packed batch the
+        // vertices of its tile ranges, i.e. of the components of its roots);
+        // single-root slots: roots at level 0 with sigma 1
+        auto reset_rows = [&](size_t v_begin, size_t v_end) {
+            for (size_t v = v_begin + (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < v_end;
+                 v += (size_t)gridDim.x * blockDim.x) {
+                constexpr int VW = RowGeom<S>::kValWord;
+                uint32_t w[R / 4];
 #pragma unroll
-            for (int q = 0; q < VW; ++q) w[q] = 0xFFFFFFFFu;  // all levels unvisited
+                for (int q = 0; q < VW; ++q) w[q] = 0xFFFFFFFFu;  // all levels unvisited
 #pragma unroll
-            for (int q = VW; q < R / 4; ++q) w[q] = 0u;
+                for (int q = VW; q < R / 4; ++q) w[q] = 0u;
 #pragma unroll
-            for (int k = 0; k < S; ++k) {
-                if (sm.roots[k] != (uint32_t)v) continue;
-                w[k >> 1] &= ~(0xFFFFu << ((k & 1) * 16));  // level 0
-                w[VW + 2 * k] = 1u;                         // sigma 1
+                for (int k = 0; k < S; ++k) {
+                    if (sm.roots[k] != (uint32_t)v) continue;
+                    w[k >> 1] &= ~(0xFFFFu << ((k & 1) * 16));  // level 0
+                    w[VW + 2 * k] = 1u;                         // sigma 1
+                }
+                uint4 *p = reinterpret_cast<uint4 *>(a.rows + v * R);
+#pragma unroll
+                for (int h = 0; h < R / 16; ++h)
+                    p[h] = make_uint4(w[4 * h], w[4 * h + 1], w[4 * h + 2], w[4 * h + 3]);
             }
-            uint4 *p = reinterpret_cast<uint4 *>(a.rows + v * R);
-#pragma unroll
-            for (int h = 0; h < R / 16; ++h) p[h] = make_uint4(w[4 * h], w[4 * h + 1], w[4 * h + 2], w[4 * h + 3]);
+        };
+        if (!packed) {
+            reset_rows(0, a.n);
+        } else {
+            const uint32_t q0 = a.xrbeg[b], q1 = a.xrbeg[b + 1];
+            for (uint32_t q = q0; q < q1; ++q) {
+                const uint2 rg = a.xrange[q];
+                const uint32_t len = ((q + 1 < q1) ? a.xrange[q + 1].y : a.xtiles[b]) - rg.y;
+                if (len) reset_rows(a.tiles[rg.x].v0, a.tiles[rg.x + len - 1].v1);
+            }
         }
         if (!grid_sync(c, nblk, wait_ns)) return;
         if (packed) {
