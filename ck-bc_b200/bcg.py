@@ -72,6 +72,8 @@ SIGNATURES = {
     "bcg_csr_generate": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(HostCSR)]),
     "bcg_csr_write_edgelist": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(HostCSR)]),
     "bcg_csr_free": (None, [ctypes.POINTER(HostCSR)]),
+    "bcg_csr_write_binary": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(HostCSR)]),
+    "bcg_csr_read_binary": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(HostCSR)]),
     "bcg_sample_sources": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, _u32p]),
     "bcg_device_count": (ctypes.c_int, []),
     "bcg_graph_create": (ctypes.c_int, [_u32p, _u32p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint32,
@@ -150,8 +152,11 @@ def _p32(a: np.ndarray):
 
 def _take_csr(h: HostCSR):
     n, nnz = h.n, h.nnz
-    offs = np.ctypeslib.as_array(h.offsets, shape=(n + 1,)).copy()
-    adj = np.ctypeslib.as_array(h.adj, shape=(max(nnz, 1),))[:nnz].copy() if nnz else np.zeros(0, np.uint32)
+    offs = np.empty(n + 1, dtype=np.uint32)
+    adj = np.empty(nnz, dtype=np.uint32)
+    ctypes.memmove(offs.ctypes.data, h.offsets, 4 * (n + 1))
+    if nnz:
+        ctypes.memmove(adj.ctypes.data, h.adj, 4 * nnz)
     lib().bcg_csr_free(ctypes.byref(h))
     return offs, adj
 
@@ -183,6 +188,19 @@ def write_edgelist(path: str, offsets: np.ndarray, adj: np.ndarray):
     adj = np.ascontiguousarray(adj, dtype=np.uint32)
     h = HostCSR(len(offsets) - 1, len(adj), _p32(offsets), _p32(adj))
     _check(lib().bcg_csr_write_edgelist(os.fsencode(path), ctypes.byref(h)))
+
+
+def write_binary(path: str, offsets: np.ndarray, adj: np.ndarray):
+    offsets = np.ascontiguousarray(offsets, dtype=np.uint32)
+    adj = np.ascontiguousarray(adj, dtype=np.uint32)
+    h = HostCSR(len(offsets) - 1, len(adj), _p32(offsets), _p32(adj) if len(adj) else None)
+    _check(lib().bcg_csr_write_binary(os.fsencode(path), ctypes.byref(h)))
+
+
+def read_binary(path: str):
+    h = HostCSR()
+    _check(lib().bcg_csr_read_binary(os.fsencode(path), ctypes.byref(h)))
+    return _take_csr(h)
 
 
 def sample_sources(n: int, k: int, seed: int) -> np.ndarray:

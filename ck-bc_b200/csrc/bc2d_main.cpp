@@ -20,7 +20,8 @@
 //     the aggregate rate (sum of component edges / kernel time / 2^20).
 // Extensions (letters unused by the reference): -s <file> source list (one id
 // per line), -F full-precision output ("%.17g" of bc/2), -G <spec> generator
-// spec (see bcg_csr_generate), -W <1|3|6> sources per batch.
+// spec (see bcg_csr_generate), -W <1|3|6> sources per batch, -B <path> binary
+// CSR cache of the -f graph (read when it exists, else written after parsing).
 #include <getopt.h>
 #include <sys/time.h>
 
@@ -65,6 +66,7 @@ static double now_us() {
            "\t\t -s <file> list of source vertices (one id per line)\n"
            "\t\t -F write bc/2 with full precision (%%.17g)\n"
            "\t\t -G <spec> generate a graph (rmat:/er:/grid: spec)\n"
+           "\t\t -B <path> binary CSR cache of the -f graph (read if present, else written)\n"
            "\t\t -W <1|3|6> sources per batch\n"
            "\n",
            pname);
@@ -83,14 +85,14 @@ int main(int argc, char *argv[]) {
     uint32_t width = 0;
     uint64_t N = 0, startv = 0;
     int64_t nbfs = 1;
-    std::string gfile, ofile, srcfile, genspec;
+    std::string gfile, ofile, srcfile, genspec, cachefile;
 
     std::string cmdline = "MPI Tasks 0\n";
     for (int i = 0; i < argc; ++i) { cmdline += " "; cmdline += argv[i]; }
     fprintf(stdout, "%s\n\n", cmdline.c_str());
 
     int opt;
-    while ((opt = getopt(argc, argv, "o:p:amhDR:Uf:n:r:S:E:N:H:s:FG:W:")) != EOF) {
+    while ((opt = getopt(argc, argv, "o:p:amhDR:Uf:n:r:S:E:N:H:s:FG:W:B:")) != EOF) {
 #define CHECKRTYPE(exitval, o)                                        \
     {                                                                 \
         if ((exitval) == gread) prexit("Unexpected option -%c!\n", o); \
@@ -144,6 +146,7 @@ int main(int argc, char *argv[]) {
             case 's': srcfile = optarg; break;
             case 'F': full = 1; break;
             case 'G': CHECKRTYPE(1, 'G'); genspec = optarg; break;
+            case 'B': cachefile = optarg; break;
             case 'W':
                 if (1 != sscanf(optarg, "%u", &width)) prexit("Invalid batch width (-W): %s\n", optarg);
                 break;
@@ -205,8 +208,18 @@ int main(int argc, char *argv[]) {
     double t0 = now_us();
     int rc;
     if (gread == 1) {
-        rc = bcg_csr_read_edgelist(gfile.c_str(), N, undirected, 1, &g);
-        if (rc) prexit("%s\n", bcg_last_error());
+        FILE *cf = cachefile.empty() ? nullptr : fopen(cachefile.c_str(), "rb");
+        if (cf) {
+            fclose(cf);
+            rc = bcg_csr_read_binary(cachefile.c_str(), &g);
+            if (rc) prexit("%s\n", bcg_last_error());
+            if (g.n != N) prexit("Cache %s holds %u vertices, not N=%" PRIu64 "\n", cachefile.c_str(), g.n, N);
+        } else {
+            rc = bcg_csr_read_edgelist(gfile.c_str(), N, undirected, 1, &g);
+            if (rc) prexit("%s\n", bcg_last_error());
+            if (!cachefile.empty() && bcg_csr_write_binary(cachefile.c_str(), &g))
+                fprintf(stderr, "warning: %s\n", bcg_last_error());
+        }
     } else {
         std::string spec = genspec;
         if (spec.empty()) {

@@ -42,6 +42,10 @@
 
 #include "bcg_common.hpp"
 
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
 namespace bcg {
 
 static thread_local std::string g_last_error;
@@ -129,50 +133,139 @@ static int build_csr(const uint64_t *pairs, uint64_t npairs, uint64_t n,
 // Edge-list reader.
 // ---------------------------------------------------------------------------
 
+// sscanf "%lu" on one field: optional leading white space and sign, then
+// decimal digits (strtoull semantics: a value past 2^64-1 saturates, a minus
+// sign negates modulo 2^64).  Returns false when there is no digit.
+static bool scan_u64(const char *&p, const char *end, uint64_t &out) {
+    while (p < end && (*p == ' ' || *p == '\t' || *p == '\r' || *p == '\v' || *p == '\f' || *p == '\n')) ++p;
+    bool neg = false;
+    if (p < end && (*p == '+' || *p == '-')) neg = (*p++ == '-');
+    if (p >= end || *p < '0' || *p > '9') return false;
+    uint64_t v = 0;
+    bool sat = false;
+    for (; p < end && *p >= '0' && *p <= '9'; ++p) {
+        const uint64_t d = (uint64_t)(*p - '0');
+        if (v > (UINT64_MAX - d) / 10) sat = true;
+        else v = v * 10 + d;
+    }
+    out = sat ? UINT64_MAX : (neg ? (uint64_t)0 - v : v);
+    return true;
+}
+
+namespace {
+// What one chunk of an edge-list file holds (lines [begin, end) of the file).
+struct EdgeChunk {
+    std::vector<uint64_t> pairs;
+    uint64_t lines = 0;                   // non-comment lines, the reference's line count
+    uint64_t bad_line = 0;                // 1-based within the chunk, 0 = none
+    uint64_t bad_u = 0, bad_v = 0;
+    std::string bad_text;
+    std::vector<std::pair<uint64_t, std::string>> echo;  // (lines before it, text)
+};
+}  // namespace
+
+static void parse_chunk(const char *b, const char *e, uint64_t n, bool echo, EdgeChunk &c) {
+    const char *ls = b;
+    while (ls < e) {
+        const char *le = static_cast<const char *>(memchr(ls, '\n', (size_t)(e - ls)));
+        if (!le) le = e;
+        const char *next = (le < e) ? le + 1 : e;
+        if (memchr(ls, '#', (size_t)(le - ls))) {
+            if (echo) {
+                const std::string line(ls, le);
+                if (line.find("Nodes:") != std::string::npos) {
+                    uint64_t nn = 0, ne = (uint64_t)-1;
+                    if (sscanf(line.c_str(), "# Nodes: %" SCNu64 " Edges: %" SCNu64, &nn, &ne) >= 1) {
+                        char buf[96];
+                        snprintf(buf, sizeof(buf), "N=%" PRIu64 " E=%" PRIu64 "\n", nn, ne);
+                        c.echo.emplace_back(c.lines, buf);
+                    }
+                }
+            }
+            ls = next;
+            continue;
+        }
+        ++c.lines;
+        const char *p = ls;
+        uint64_t u, v;
+        // "%lu %lu": a malformed line is skipped (the reference would keep the
+        // previous line's values)
+        if (scan_u64(p, le, u) && scan_u64(p, le, v)) {
+            if (u >= n || v >= n) {
+                c.bad_line = c.lines;
+                c.bad_u = u;
+                c.bad_v = v;
+                c.bad_text.assign(ls, le);
+                while (!c.bad_text.empty() && c.bad_text.back() == '\r') c.bad_text.pop_back();
+                return;
+            }
+            c.pairs.push_back(u);
+            c.pairs.push_back(v);
+        }
+        ls = next;
+    }
+}
+
+// Reads the whole file, cuts it into chunks at line ends and parses them in
+// parallel; echo lines, the first bad line and the pairs come out in file order.
 static int read_edgelist(const char *path, uint64_t n, bool undirected, bool echo,
                          std::vector<uint64_t> &pairs) {
-    FILE *fp = fopen(path, "r");
-    if (!fp) return set_error(BCG_ERR_IO, "Cannot open file %s...", path);
+    (void)undirected;
     // Lines are parsed the way read_graph does it (bc2d.c:214-247): a line
     // that contains '#' anywhere is a comment; otherwise two unsigned decimal
     // integers are read (sscanf "%lu %lu").  Lines are read whole, so lines
     // longer than the reference's MAX_LINE=1024 buffer are not split.
-    std::string line;
-    char buf[4096];
-    uint64_t lineno = 0;
-    int rc = BCG_OK;
-    while (fgets(buf, sizeof(buf), fp)) {
-        line.assign(buf);
-        while (!line.empty() && line.back() != '\n' && fgets(buf, sizeof(buf), fp)) line.append(buf);
-        if (line.find('#') != std::string::npos) {
-            if (echo && line.find("Nodes:") != std::string::npos) {
-                uint64_t nn = 0, ne = (uint64_t)-1;
-                if (sscanf(line.c_str(), "# Nodes: %" SCNu64 " Edges: %" SCNu64, &nn, &ne) >= 1)
-                    fprintf(stdout, "N=%" PRIu64 " E=%" PRIu64 "\n", nn, ne);
-            }
-            continue;
-        }
-        if (line.empty() || line[0] == '\0') continue;
-        ++lineno;
-        uint64_t u, v;
-        if (sscanf(line.c_str(), "%" SCNu64 " %" SCNu64, &u, &v) != 2) {
-            // The reference keeps the previous values on a short parse; a blank
-            // or malformed line is skipped here instead.
-            continue;
-        }
-        if (u >= n || v >= n) {
-            while (!line.empty() && (line.back() == '\n' || line.back() == '\r')) line.pop_back();
-            rc = set_error(BCG_ERR_IO,
-                           "In file %s line %" PRIu64 " found invalid edge in %s for N=%" PRIu64
-                           ": (%" PRIu64 ", %" PRIu64 ")", path, lineno, line.c_str(), n, u, v);
-            break;
-        }
-        pairs.push_back(u);
-        pairs.push_back(v);
+    FILE *fp = fopen(path, "rb");
+    if (!fp) return set_error(BCG_ERR_IO, "Cannot open file %s...", path);
+    std::vector<char> buf;
+    if (fseek(fp, 0, SEEK_END) == 0) {
+        const long sz = ftell(fp);
+        if (sz > 0) buf.resize((size_t)sz);
+        rewind(fp);
+        if (sz > 0) buf.resize(fread(buf.data(), 1, buf.size(), fp));
+    } else {  // not seekable: read in pieces
+        char tmp[1 << 16];
+        size_t got;
+        while ((got = fread(tmp, 1, sizeof(tmp), fp)) > 0) buf.insert(buf.end(), tmp, tmp + got);
     }
+    const bool err = ferror(fp);
     fclose(fp);
-    (void)undirected;
-    return rc;
+    if (err) return set_error(BCG_ERR_IO, "read error on %s", path);
+    const char *base = buf.data(), *end = base + buf.size();
+    int nt = 1;
+#ifdef _OPENMP
+    nt = omp_get_max_threads();
+#endif
+    const size_t want = (size_t)nt * 4;
+    std::vector<const char *> cut{base};
+    for (size_t i = 1; i < want; ++i) {
+        const char *q = base + buf.size() * i / want;
+        if (q <= cut.back()) continue;
+        const char *nl = static_cast<const char *>(memchr(q, '\n', (size_t)(end - q)));
+        if (!nl) break;
+        if (nl + 1 > cut.back()) cut.push_back(nl + 1);
+    }
+    cut.push_back(end);
+    const size_t nc = cut.size() - 1;
+    std::vector<EdgeChunk> ch(nc);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long i = 0; i < (long)nc; ++i) parse_chunk(cut[i], cut[i + 1], n, echo, ch[i]);
+    uint64_t before = 0, total = 0;
+    for (size_t i = 0; i < nc; ++i) {
+        for (const auto &ev : ch[i].echo)
+            if (!ch[i].bad_line || ev.first < ch[i].bad_line) fputs(ev.second.c_str(), stdout);
+        if (ch[i].bad_line)
+            return set_error(BCG_ERR_IO,
+                             "In file %s line %" PRIu64 " found invalid edge in %s for N=%" PRIu64
+                             ": (%" PRIu64 ", %" PRIu64 ")", path, before + ch[i].bad_line,
+                             ch[i].bad_text.c_str(), n, ch[i].bad_u, ch[i].bad_v);
+        before += ch[i].lines;
+        total += ch[i].pairs.size();
+    }
+    pairs.clear();
+    pairs.reserve(total);
+    for (auto &c : ch) pairs.insert(pairs.end(), c.pairs.begin(), c.pairs.end());
+    return BCG_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -453,6 +546,77 @@ int bcg_csr_write_edgelist(const char *path, const bcg_host_csr *g) {
             if (v < g->adj[e]) fprintf(fp, "%u %u\n", v, g->adj[e]);
     int bad = ferror(fp);
     if (fclose(fp) != 0 || bad) return set_error(BCG_ERR_IO, "write to %s failed", path);
+    return BCG_OK;
+}
+
+// Binary CSR cache: "BCGCSR01", then n, nnz and an FNV-1a checksum of the
+// two arrays (all little-endian uint64), then offsets[n+1] and adj[nnz] as
+// uint32.  Reading it skips the text parse and the normalisation.
+static uint64_t fnv1a_words(const uint32_t *w, uint64_t count, uint64_t h) {
+    for (uint64_t i = 0; i < count; ++i) {
+        h ^= w[i];
+        h *= 0x100000001B3ull;
+    }
+    return h;
+}
+
+static const char kCsrMagic[8] = {'B', 'C', 'G', 'C', 'S', 'R', '0', '1'};
+
+int bcg_csr_write_binary(const char *path, const bcg_host_csr *g) {
+    clear_error();
+    if (!path || !g || !g->offsets || (g->nnz && !g->adj)) return set_error(BCG_ERR_ARG, "null argument");
+    uint64_t h = fnv1a_words(g->offsets, (uint64_t)g->n + 1, 0xCBF29CE484222325ull);
+    h = fnv1a_words(g->adj, g->nnz, h);
+    const uint64_t head[3] = {g->n, g->nnz, h};
+    FILE *fp = fopen(path, "wb");
+    if (!fp) return set_error(BCG_ERR_IO, "Cannot open file %s...", path);
+    bool ok = fwrite(kCsrMagic, 1, 8, fp) == 8 && fwrite(head, 8, 3, fp) == 3 &&
+              fwrite(g->offsets, 4, (size_t)g->n + 1, fp) == (size_t)g->n + 1 &&
+              (g->nnz == 0 || fwrite(g->adj, 4, g->nnz, fp) == g->nnz);
+    ok = (fclose(fp) == 0) && ok;
+    if (!ok) return set_error(BCG_ERR_IO, "write to %s failed", path);
+    return BCG_OK;
+}
+
+int bcg_csr_read_binary(const char *path, bcg_host_csr *out) {
+    clear_error();
+    if (!path || !out) return set_error(BCG_ERR_ARG, "null argument");
+    *out = bcg_host_csr{};
+    FILE *fp = fopen(path, "rb");
+    if (!fp) return set_error(BCG_ERR_IO, "Cannot open file %s...", path);
+    char magic[8];
+    uint64_t head[3];
+    if (fread(magic, 1, 8, fp) != 8 || memcmp(magic, kCsrMagic, 8) != 0 || fread(head, 8, 3, fp) != 3) {
+        fclose(fp);
+        return set_error(BCG_ERR_IO, "%s is not a binary CSR cache", path);
+    }
+    const uint64_t n = head[0], nnz = head[1];
+    if (n == 0 || n > 0xFFFFFFFEull || nnz > 0xFFFFFFFFull) {
+        fclose(fp);
+        return set_error(BCG_ERR_IO, "%s: bad sizes n=%" PRIu64 " nnz=%" PRIu64, path, n, nnz);
+    }
+    uint32_t *offs = (uint32_t *)malloc((n + 1) * sizeof(uint32_t));
+    uint32_t *adj = (uint32_t *)malloc(std::max<uint64_t>(1, nnz) * sizeof(uint32_t));
+    bool ok = offs && adj && fread(offs, 4, n + 1, fp) == n + 1 && (nnz == 0 || fread(adj, 4, nnz, fp) == nnz);
+    char extra;
+    ok = ok && fread(&extra, 1, 1, fp) == 0;  // nothing after the arrays
+    fclose(fp);
+    if (ok) {
+        uint64_t h = fnv1a_words(offs, n + 1, 0xCBF29CE484222325ull);
+        h = fnv1a_words(adj, nnz, h);
+        ok = (h == head[2]) && offs[0] == 0 && offs[n] == nnz;
+        for (uint64_t v = 0; ok && v < n; ++v) ok = offs[v] <= offs[v + 1];
+        for (uint64_t e = 0; ok && e < nnz; ++e) ok = adj[e] < n;
+    }
+    if (!ok) {
+        free(offs);
+        free(adj);
+        return set_error(BCG_ERR_IO, "%s: truncated or corrupt binary CSR cache", path);
+    }
+    out->n = (uint32_t)n;
+    out->nnz = nnz;
+    out->offsets = offs;
+    out->adj = adj;
     return BCG_OK;
 }
 

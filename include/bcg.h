@@ -86,6 +86,13 @@ int bcg_csr_generate(const char *spec, bcg_host_csr *out);
  * once, u < v, with a "# Nodes: N Edges: E" header). */
 int bcg_csr_write_edgelist(const char *path, const bcg_host_csr *g);
 
+/* Binary CSR cache (fast ingest; no counterpart in the reference, which
+ * parses the text file on every run, bc2d.c:214-247): "BCGCSR01", n, nnz
+ * and a checksum, then offsets[n+1] and adj[nnz] as uint32.  Reading checks
+ * the checksum and the CSR invariants (BCG_ERR_IO when they fail). */
+int bcg_csr_write_binary(const char *path, const bcg_host_csr *g);
+int bcg_csr_read_binary(const char *path, bcg_host_csr *out);
+
 void bcg_csr_free(bcg_host_csr *g);
 
 /* k distinct vertices drawn uniformly from [0, n) with the given seed

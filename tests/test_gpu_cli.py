@@ -109,3 +109,22 @@ def test_reference_host_driver_over_compat(graph_file, tmp_path):
     ref, _ = oracle.bc(offs, adj, np.arange(200, dtype=np.uint32))
     # float32 get_bc and "%.2f" output (cuda_kernels.cu:1039-1041, bc2d.c:1065)
     assert np.all(np.abs(vals - ref / 2) <= 0.005 + 2e-7 * np.abs(ref))
+
+
+def test_cli_binary_cache(graph_file, tmp_path):
+    """-B writes the binary CSR cache on the first run and reads it on the
+    second (the text file is then not needed); both runs give the same file."""
+    path, offs, adj = graph_file
+    n = len(offs) - 1
+    cache = str(tmp_path / "g.bcsr")
+    outs = []
+    for i, f in enumerate([path, str(tmp_path / "absent.txt")]):
+        out = str(tmp_path / f"res{i}")
+        r = subprocess.run([BC2D, "-p", "1x1", "-f", f, "-n", str(n), "-N", "64", "-B", cache, "-o", out, "-F"],
+                           capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        assert os.path.exists(cache)
+        outs.append(_read_result(out + "_1X1_0.log")[2])
+    np.testing.assert_array_equal(outs[0], outs[1])
+    ref, _ = oracle.bc(offs, adj, np.arange(64, dtype=np.uint32))
+    np.testing.assert_allclose(outs[1], ref / 2, rtol=1e-9, atol=1e-9)
