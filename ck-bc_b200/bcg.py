@@ -30,6 +30,10 @@ ERR_NOGPU = -9
 PRUNE_DEGREE1 = 0x1
 DIRECTED = 0x2
 
+SIGMA_AUTO = 0
+SIGMA_EXACT = 1
+SIGMA_EXTENDED = 2
+
 NOALLOC_MAX_VERTICES = 65536
 NOALLOC_MAX_ADJ = 1048576
 NOALLOC_MAX_SOURCES = 65536
@@ -51,7 +55,7 @@ class Stats(ctypes.Structure):
                 ("teps_edges", ctypes.c_uint64), ("visited", ctypes.c_uint64),
                 ("comp_vertices", ctypes.c_uint64),
                 ("max_depth", ctypes.c_uint32), ("batch_width", ctypes.c_uint32),
-                ("kernel_ms", ctypes.c_double)]
+                ("kernel_ms", ctypes.c_double), ("extended_sigma", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -99,6 +103,8 @@ SIGNATURES = {
     "bcg_run_weighted": (ctypes.c_int, [ctypes.c_void_p, _u32p, _f64p, _u32p, ctypes.c_uint64,
                                         ctypes.POINTER(Stats)]),
     "bcg_set_batch_width": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32]),
+    "bcg_set_sigma_mode": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "bcg_single_source_ext": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, _i32p, _u64p, _f64p]),
     "bcg_batch_create": (ctypes.c_int, [ctypes.c_uint32, ctypes.POINTER(_u32p), ctypes.POINTER(_u32p), _u32p,
                                         ctypes.POINTER(ctypes.c_void_p)]),
     "bcg_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
@@ -203,6 +209,16 @@ def read_binary(path: str):
     return _take_csr(h)
 
 
+def ext_log2(raw: np.ndarray) -> np.ndarray:
+    """log2 of extended-encoding values ((2^48 + f) * 2^(E - 32816)); -inf for 0."""
+    raw = np.asarray(raw, dtype=np.uint64)
+    e = (raw >> np.uint64(48)).astype(np.int64)
+    f = (raw & np.uint64((1 << 48) - 1)).astype(np.float64)
+    out = np.log2(1.0 + f / 2.0**48) + (e - 32816 + 48).astype(np.float64)
+    out[raw == 0] = -np.inf
+    return out
+
+
 def sample_sources(n: int, k: int, seed: int) -> np.ndarray:
     out = np.zeros(k, dtype=np.uint32)
     _check(lib().bcg_sample_sources(n, k, seed, _p32(out)))
@@ -293,6 +309,19 @@ class Graph:
 
     def set_batch_width(self, w: int):
         _check(lib().bcg_set_batch_width(self.h, w))
+
+    def set_sigma_mode(self, mode: int):
+        _check(lib().bcg_set_sigma_mode(self.h, mode))
+
+    def single_source_ext(self, src: int):
+        """-> (level, sigma as float log2 values (-inf for 0), delta); sigma
+        is decoded from the extended encoding."""
+        lvl = np.zeros(self.n, dtype=np.int32)
+        raw = np.zeros(self.n, dtype=np.uint64)
+        dl = np.zeros(self.n, dtype=np.float64)
+        _check(lib().bcg_single_source_ext(self.h, src, lvl.ctypes.data_as(_i32p), raw.ctypes.data_as(_u64p),
+                                           dl.ctypes.data_as(_f64p)))
+        return lvl, ext_log2(raw), dl
 
 
 class Batch:

@@ -189,7 +189,7 @@ static void graph_free(bcg_graph *g) {
     cudaFree(g->d_anchor); cudaFree(g->d_reach); cudaFree(g->d_bc);
     cudaFree(g->d_tiles); cudaFree(g->d_hub_acc); cudaFree(g->d_hub_cnt);
     cudaFree(g->d_tile_of); cudaFree(g->d_tmark); cudaFree(g->d_lists);
-    cudaFree(g->d_lbase); cudaFree(g->d_lcnt); cudaFree(g->d_ulist);
+    cudaFree(g->d_lbase); cudaFree(g->d_lcnt); cudaFree(g->d_ulist); cudaFree(g->d_bc_save);
     cudaFree(g->d_rows); cudaFree(g->d_ctrl);
     cudaFree(g->d_roots); cudaFree(g->d_pend); cudaFree(g->d_mult); cudaFree(g->d_rstat);
     if (g->ev0) cudaEventDestroy(g->ev0);
@@ -432,54 +432,83 @@ static int run_plan(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *
         a.trace_cap = trace_cap;
         a.trace_cnt = d_tcnt;
     }
-    CK(cudaEventRecord(g->ev0, st));
-    // tile marks key on the batch index modulo 2^16, so one launch runs at most
-    // 65535 batches and the marks are cleared before every launch
-    const uint64_t per_launch = 65535;
-    for (uint64_t b0 = 0; b0 < nbatch; b0 += per_launch) {
-        const uint64_t nb = std::min(per_launch, nbatch - b0);
-        CK(cudaMemsetAsync(g->d_ctrl, 0, sizeof(Ctrl), st));
-        CK(cudaMemcpyAsync(&g->d_ctrl->wait_ns, &g->wait_ns, sizeof(unsigned long long), cudaMemcpyHostToDevice, st));
-        CK(cudaMemsetAsync(g->d_tmark, 0, (size_t)std::max(1u, g->ntiles) * sizeof(uint32_t), st));
-        a.roots = g->d_roots + b0 * S;
-        a.mult = g->d_mult + b0 * S;
-        a.pend = g->d_pend + b0 * S;
-        a.rstat = g->d_rstat + b0 * S;
-        a.nbatch = (uint32_t)nb;
-        int grid = 0;
-        rc = launch_sweep((int)S, a, st, &grid);
-        if (rc) return rc;
-        if (b0 + nb < nbatch) {
-            // errors of this launch are read before the control block is reused
+    // Sigma is exact uint64 unless the graph runs in extended mode; in the
+    // automatic mode a run whose counts overflow is redone in extended mode
+    // from a saved copy of the accumulators.
+    const bool autoext = g->sigma_mode == 0;
+    bool ext = g->sigma_mode == 2;
+    if (autoext) {
+        if (!g->d_bc_save) CK(cudaMalloc(&g->d_bc_save, (size_t)g->n * sizeof(double)));
+        CK(cudaMemcpyAsync(g->d_bc_save, g->d_bc, (size_t)g->n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    }
+    for (;;) {
+        CK(cudaEventRecord(g->ev0, st));
+        // tile marks key on the batch index modulo 2^16, so one launch runs at
+        // most 65535 batches and the marks are cleared before every launch
+        const uint64_t per_launch = 65535;
+        for (uint64_t b0 = 0; b0 < nbatch; b0 += per_launch) {
+            const uint64_t nb = std::min(per_launch, nbatch - b0);
+            CK(cudaMemsetAsync(g->d_ctrl, 0, sizeof(Ctrl), st));
+            CK(cudaMemcpyAsync(&g->d_ctrl->wait_ns, &g->wait_ns, sizeof(unsigned long long), cudaMemcpyHostToDevice,
+                               st));
+            CK(cudaMemsetAsync(g->d_tmark, 0, (size_t)std::max(1u, g->ntiles) * sizeof(uint32_t), st));
+            a.roots = g->d_roots + b0 * S;
+            a.mult = g->d_mult + b0 * S;
+            a.pend = g->d_pend + b0 * S;
+            a.rstat = g->d_rstat + b0 * S;
+            a.nbatch = (uint32_t)nb;
+            int grid = 0;
+            rc = launch_sweep((int)S, a, st, &grid, ext);
+            if (rc) return rc;
+            if (b0 + nb < nbatch) {
+                // errors of this launch are read before the control block is reused
+                CK(cudaStreamSynchronize(st));
+                Ctrl c{};
+                CK(cudaMemcpy(&c, g->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+                if (c.error || c.overflow) break;
+            }
+        }
+        CK(cudaEventRecord(g->ev1, st));
+        if (d_trace) {
             CK(cudaStreamSynchronize(st));
-            Ctrl c{};
-            CK(cudaMemcpy(&c, g->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
-            if (c.error || c.overflow) break;
+            unsigned int cnt = 0;
+            CK(cudaMemcpy(&cnt, d_tcnt, sizeof(cnt), cudaMemcpyDeviceToHost));
+            std::vector<TraceRec> recs(cnt);
+            if (cnt) CK(cudaMemcpy(recs.data(), d_trace, cnt * sizeof(TraceRec), cudaMemcpyDeviceToHost));
+            CK(cudaMemsetAsync(d_tcnt, 0, sizeof(unsigned int), st));
+            if (FILE *f = fopen(trace_path, "a")) {
+                fprintf(f, "# width %u roots %zu tiles %u\n", S, (size_t)nroots, g->ntiles);
+                for (const TraceRec &r : recs)
+                    fprintf(f, "%u,%u,%u,%u,%llu,%llu\n", r.batch, r.kind, r.level, r.nwork, r.disc, r.t_ns);
+                fclose(f);
+            }
         }
-    }
-    CK(cudaEventRecord(g->ev1, st));
-    if (d_trace) {
+        if (!stats && !debug && !autoext) break;
         CK(cudaStreamSynchronize(st));
-        unsigned int cnt = 0;
-        CK(cudaMemcpy(&cnt, d_tcnt, sizeof(cnt), cudaMemcpyDeviceToHost));
-        std::vector<TraceRec> recs(cnt);
-        if (cnt) CK(cudaMemcpy(recs.data(), d_trace, cnt * sizeof(TraceRec), cudaMemcpyDeviceToHost));
-        cudaFree(d_trace);
-        cudaFree(d_tcnt);
-        if (FILE *f = fopen(trace_path, "a")) {
-            fprintf(f, "# width %u roots %zu tiles %u\n", S, (size_t)nroots, g->ntiles);
-            for (const TraceRec &r : recs)
-                fprintf(f, "%u,%u,%u,%u,%llu,%llu\n", r.batch, r.kind, r.level, r.nwork, r.disc, r.t_ns);
-            fclose(f);
+        Ctrl c{};
+        CK(cudaMemcpy(&c, g->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+        if (c.error && c.error != BCG_ERR_OVERFLOW) {
+            cudaFree(d_trace);
+            cudaFree(d_tcnt);
+            return set_error(c.error, "device reported error %d (%s)", c.error,
+                             c.error == BCG_ERR_TIMEOUT ? "a bounded wait gave up" : "level limit exceeded");
         }
+        if (c.overflow || c.error == BCG_ERR_OVERFLOW) {
+            if (autoext && !ext) {
+                CK(cudaMemcpyAsync(g->d_bc, g->d_bc_save, (size_t)g->n * sizeof(double), cudaMemcpyDeviceToDevice,
+                                   st));
+                ext = true;
+                continue;
+            }
+            cudaFree(d_trace);
+            cudaFree(d_tcnt);
+            return set_error(BCG_ERR_OVERFLOW, "a shortest-path count exceeded 2^64");
+        }
+        break;
     }
-    if (!stats && !debug) return BCG_OK;
-    CK(cudaStreamSynchronize(st));
-    Ctrl c{};
-    CK(cudaMemcpy(&c, g->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
-    if (c.error) return set_error(c.error, "device reported error %d (%s)", c.error,
-                                  c.error == BCG_ERR_TIMEOUT ? "a bounded wait gave up" : "level limit exceeded");
-    if (c.overflow) return set_error(BCG_ERR_OVERFLOW, "a shortest-path count exceeded 2^64");
+    cudaFree(d_trace);
+    cudaFree(d_tcnt);
+    if (!stats) return BCG_OK;
     if (stats) {
         std::vector<RootStat> rs(slots);
         CK(cudaMemcpy(rs.data(), g->d_rstat, slots * sizeof(RootStat), cudaMemcpyDeviceToHost));
@@ -500,6 +529,7 @@ static int run_plan(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *
         stats->max_depth = md;
         stats->batch_width = S;
         stats->kernel_ms = ms;
+        stats->extended_sigma = ext ? 1u : 0u;
     }
     return BCG_OK;
 }
@@ -560,9 +590,10 @@ int check_ctrl(bcg_graph *g, cudaStream_t st) {
     CK(cudaStreamSynchronize(st));
     Ctrl c{};
     CK(cudaMemcpy(&c, g->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+    if (c.overflow || c.error == BCG_ERR_OVERFLOW)
+        return set_error(BCG_ERR_OVERFLOW, "a shortest-path count exceeded 2^64");
     if (c.error) return set_error(c.error, "device reported error %d (%s)", c.error,
                                   c.error == BCG_ERR_TIMEOUT ? "a bounded wait gave up" : "level limit exceeded");
-    if (c.overflow) return set_error(BCG_ERR_OVERFLOW, "a shortest-path count exceeded 2^64");
     return BCG_OK;
 }
 
@@ -706,7 +737,7 @@ int bcg_bc_csr(const uint32_t *offsets, const uint32_t *adj, uint32_t n, uint64_
     return rc;
 }
 
-int bcg_single_source(bcg_graph *g, uint32_t src, int32_t *level, uint64_t *sigma, double *delta) {
+static int single_source_impl(bcg_graph *g, uint32_t src, int32_t *level, uint64_t *sigma, double *delta) {
     clear_error();
     if (!g) return set_error(BCG_ERR_ARG, "null handle");
     if (src >= g->n) return set_error(BCG_ERR_ARG, "source %u >= n=%u", src, g->n);
@@ -750,6 +781,32 @@ int bcg_single_source(bcg_graph *g, uint32_t src, int32_t *level, uint64_t *sigm
     cudaMemcpy(g->d_bc, d_save, n * sizeof(double), cudaMemcpyDeviceToDevice);
     cleanup();
     return rc;
+}
+
+int bcg_single_source(bcg_graph *g, uint32_t src, int32_t *level, uint64_t *sigma, double *delta) {
+    if (!g) return set_error(BCG_ERR_ARG, "null handle");
+    const int mode = g->sigma_mode;
+    g->sigma_mode = 1;  // uint64 counts: an overflow is an error here
+    const int rc = single_source_impl(g, src, level, sigma, delta);
+    g->sigma_mode = mode;
+    return rc;
+}
+
+int bcg_single_source_ext(bcg_graph *g, uint32_t src, int32_t *level, uint64_t *sigma_ext, double *delta) {
+    if (!g) return set_error(BCG_ERR_ARG, "null handle");
+    const int mode = g->sigma_mode;
+    g->sigma_mode = 2;
+    const int rc = single_source_impl(g, src, level, sigma_ext, delta);
+    g->sigma_mode = mode;
+    return rc;
+}
+
+int bcg_set_sigma_mode(bcg_graph *g, int mode) {
+    clear_error();
+    if (!g) return set_error(BCG_ERR_ARG, "null handle");
+    if (mode < 0 || mode > 2) return set_error(BCG_ERR_ARG, "sigma mode %d not in {0, 1, 2}", mode);
+    g->sigma_mode = mode;
+    return BCG_OK;
 }
 
 int bcg_graph_pruning(bcg_graph *g, uint32_t *anchor, uint32_t *reach) {

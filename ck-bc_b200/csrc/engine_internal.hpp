@@ -45,13 +45,16 @@ struct bcg_graph {
     uint32_t tile_vcap = kTileVerts, tile_ecap = kTileEdges;  // tile shape (autotuned by batches)
     std::vector<uint32_t> tile_breaks;  // sorted vertices where a new tile must start
     float ratio = 0.2f;
+    int sigma_mode = 0;               // 0 auto (exact, extended on overflow), 1 exact only, 2 extended
+    double *d_bc_save = nullptr;      // accumulators before an automatic-mode run
     unsigned long long wait_ns = kDefaultWaitNs;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
 namespace bcg {
 
-int launch_sweep(int S, const BatchArgs &a, cudaStream_t st, int *grid_out);
+// ext: sigma and X as extended-range numbers (ext64.cuh) instead of uint64 / double
+int launch_sweep(int S, const BatchArgs &a, cudaStream_t st, int *grid_out, bool ext = false);
 
 // Component-packed batches already on the device (see BatchArgs::xbeg).
 struct PackedRun {

@@ -27,7 +27,7 @@
 
 namespace bcg {
 
-int launch_sweep(int S, const BatchArgs &a, cudaStream_t st, int *grid_out);
+int launch_sweep(int S, const BatchArgs &a, cudaStream_t st, int *grid_out, bool ext = false);
 
 namespace {
 
@@ -386,9 +386,10 @@ extern "C" int bcg_bc_noalloc(const uint32_t *d_offsets, const uint32_t *d_adj, 
     int flags[2] = {0, 0};  // Ctrl::error, Ctrl::overflow
     NA_CK(cudaMemcpyAsync(flags, &d_ctrl->error, sizeof(flags), cudaMemcpyDeviceToHost, st));
     NA_CK(cudaStreamSynchronize(st));
+    if (flags[1] || flags[0] == BCG_ERR_OVERFLOW)
+        return set_error(BCG_ERR_OVERFLOW, "a shortest-path count exceeded 2^64");
     if (flags[0])
         return set_error(flags[0], "device reported error %d (%s)", flags[0],
                          flags[0] == BCG_ERR_TIMEOUT ? "a bounded wait gave up" : "level limit exceeded");
-    if (flags[1]) return set_error(BCG_ERR_OVERFLOW, "a shortest-path count exceeded 2^64");
     return BCG_OK;
 }

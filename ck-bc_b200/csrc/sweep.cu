@@ -46,6 +46,7 @@
 #include "bcg.h"
 #include "bcg_common.hpp"
 #include "engine.cuh"
+#include "ext64.cuh"
 
 namespace bcg {
 
@@ -363,24 +364,60 @@ __device__ __forceinline__ void flush_counts(WarpSmem<S> &ws, const LaneCounts<S
     __syncwarp();
 }
 
-template <int S, int MODE>
+// A wrapped uint64 sum: flag it and stop the launch at the next barrier (the
+// host then fails the run or redoes it with extended counts).
+__device__ __forceinline__ void flag_overflow(Ctrl *c) {
+    c->overflow = 1;
+    atomicCAS(&c->error, 0, BCG_ERR_OVERFLOW);
+}
+
+// Value arithmetic of a sweep.  Forward sweeps sum sigma values, backward
+// sweeps sum X = (1 + delta) / sigma values; with EXT both are extended-range
+// numbers (ext64.cuh), otherwise sigma is an exact uint64 (a wrapped sum sets
+// the overflow flag) and X a double.
+template <bool EXT, int MODE>
+__device__ __forceinline__ unsigned long long vsum(unsigned long long x, unsigned long long y, const BatchArgs &a) {
+    if (EXT) return ext_add(x, y);
+    if (MODE == kBwd)
+        return (unsigned long long)__double_as_longlong(__longlong_as_double((long long)x) +
+                                                        __longlong_as_double((long long)y));
+    const unsigned long long t = x + y;
+    if (t < y) flag_overflow(a.ctrl);
+    return t;
+}
+
+// *p += y atomically (p in global or shared memory).  The extended form is a
+// compare-and-swap retry loop: each failed attempt means another thread's add
+// went through, so the loop always ends.
+template <bool EXT, int MODE>
+__device__ __forceinline__ void vatomic(unsigned long long *p, unsigned long long y, const BatchArgs &a) {
+    if (EXT) {
+        unsigned long long old = *reinterpret_cast<volatile unsigned long long *>(p), seen;
+        do {
+            seen = old;
+            old = atomicCAS(p, seen, ext_add(seen, y));
+        } while (old != seen);
+    } else if (MODE == kBwd) {
+        atomicAdd(reinterpret_cast<double *>(p), __longlong_as_double((long long)y));
+    } else {
+        const unsigned long long old = atomicAdd(p, y);
+        if (old + y < y) flag_overflow(a.ctrl);
+    }
+}
+
+template <int S, int MODE, bool EXT>
 __device__ __forceinline__ void flush_run(const BatchArgs &a, WarpSmem<S> &ws, uint32_t j,
                                           unsigned long long (&run)[S]) {
 #pragma unroll
     for (int k = 0; k < S; ++k) {
         if (!run[k]) continue;
-        if (MODE == kFwdPull) {
-            const unsigned long long old = atomicAdd(&ws.acc[j][k], run[k]);
-            if (old + run[k] < run[k]) a.ctrl->overflow = 1;
-        } else {
-            atomicAdd(reinterpret_cast<double *>(&ws.acc[j][k]), __longlong_as_double((long long)run[k]));
-        }
+        vatomic<EXT, MODE>(&ws.acc[j][k], run[k], a);
         run[k] = 0ull;
     }
 }
 
 // One tile (or one part of a split tile), processed by one warp.
-template <int S, int MODE>
+template <int S, int MODE, bool EXT>
 __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint32_t ti, const Tile &T,
                           uint32_t part, const SweepCtx &x) {
     constexpr int R = RowGeom<S>::kBytes;
@@ -518,9 +555,7 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
                             }
                         }
                         if (take) {
-                            const unsigned long long s = ws.own[jj[q]][k];
-                            const unsigned long long old = atomicAdd(val_at<S>(wrow, k), s);
-                            if (old + s < s) a.ctrl->overflow = 1;
+                            vatomic<EXT, kFwdPull>(val_at<S>(wrow, k), ws.own[jj[q]][k], a);
                         }
                     }
                     if (claimed_any) app = claim_tile(a, wv, x.key_next);
@@ -557,7 +592,7 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
                     const int idx = r * E + q;
                     if (i0 + idx >= i1) continue;
                     if (jj[idx] != runj) {
-                        flush_run<S, MODE>(a, ws, runj, run);
+                        flush_run<S, MODE, EXT>(a, ws, runj, run);
                         runj = jj[idx];
                     }
                     const uint32_t jm = ws.mask[jj[idx]];
@@ -570,20 +605,11 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
 #pragma unroll
                     for (int k = 0; k < S; ++k) {
                         if (!((jm >> k) & 1u) || w_lvl(wr, k) != want) continue;
-                        const unsigned long long xv = w_val<S>(wr, k);
-                        if (MODE == kFwdPull) {
-                            const unsigned long long t = run[k] + xv;
-                            if (t < xv) a.ctrl->overflow = 1;
-                            run[k] = t;
-                        } else {
-                            const double t =
-                                __longlong_as_double((long long)run[k]) + __longlong_as_double((long long)xv);
-                            run[k] = (unsigned long long)__double_as_longlong(t);
-                        }
+                        run[k] = vsum<EXT, MODE>(run[k], w_val<S>(wr, k), a);
                     }
                 }
             }
-            if (i0 < i1) flush_run<S, MODE>(a, ws, runj, run);
+            if (i0 < i1) flush_run<S, MODE, EXT>(a, ws, runj, run);
         }
     }
     __syncwarp();
@@ -594,13 +620,7 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
         const uint32_t hm = ws.mask[0];
         unsigned long long *hacc = a.hub_acc + (size_t)T.hub * S;
         if (lane < (unsigned)S && ((hm >> lane) & 1u)) {
-            const unsigned long long xa = ws.acc[0][lane];
-            if (MODE == kFwdPull) {
-                const unsigned long long old = atomicAdd(hacc + lane, xa);
-                if (old + xa < xa) a.ctrl->overflow = 1;
-            } else {
-                atomicAdd(reinterpret_cast<double *>(hacc + lane), __longlong_as_double((long long)xa));
-            }
+            vatomic<EXT, MODE>(hacc + lane, ws.acc[0][lane], a);
         }
         __threadfence();
         __syncwarp();
@@ -640,11 +660,20 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
 #pragma unroll
             for (int k = 0; k < S; ++k) {
                 if (!((m >> k) & 1u)) continue;
-                const double sig = (double)ws.own[lane][k];
-                const double acc = __longlong_as_double((long long)ws.acc[lane][k]);
-                const double delta = reach + sig * acc;
-                const double xo = (1.0 + delta) / sig;
-                *val_at<S>(vrow, k) = (unsigned long long)__double_as_longlong(xo);
+                double delta;
+                if (EXT) {
+                    // sigma * sum X is a dependency count (in double range)
+                    // even where sigma and X are not
+                    const unsigned long long sig = ws.own[lane][k];
+                    delta = reach + ext_to_double(ext_mul(sig, ws.acc[lane][k]));
+                    *val_at<S>(vrow, k) = ext_div(1.0 + delta, sig);
+                } else {
+                    const double sig = (double)ws.own[lane][k];
+                    const double acc = __longlong_as_double((long long)ws.acc[lane][k]);
+                    delta = reach + sig * acc;
+                    const double xo = (1.0 + delta) / sig;
+                    *val_at<S>(vrow, k) = (unsigned long long)__double_as_longlong(xo);
+                }
                 if (d > 0) add += sm.mult[k] * delta;
                 if (a.dbg_delta) a.dbg_delta[v] = delta;
             }
@@ -672,8 +701,8 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
 // working instead of waiting at the sweep's barrier.
 // With no list and a range table, item i is tile ranges[r].x + (i - ranges[r].y)
 // for the last range r with ranges[r].y <= i (nranges ranges, increasing .y).
-template <int S>
-__device__ void run_sweep(const BatchArgs &a, Smem<S> &sm, const SweepCtx &x, const uint32_t *list,
+template <int S, bool EXT>
+__device__ __forceinline__ void run_sweep(const BatchArgs &a, Smem<S> &sm, const SweepCtx &x, const uint32_t *list,
                           unsigned long long start, uint32_t nwork, unsigned long long ring,
                           const uint2 *ranges = nullptr, uint32_t nranges = 0) {
     const unsigned wid = threadIdx.x >> 5;
@@ -722,9 +751,9 @@ __device__ void run_sweep(const BatchArgs &a, Smem<S> &sm, const SweepCtx &x, co
         ti1 = ti2;
         it2 = (it2 < nitems) ? grab() : nitems;
         if (it2 < nitems) ti2 = item_tile(it2);
-        if (x.mode == kFwdPush) warp_tile<S, kFwdPush>(a, sm, ws, ti, T, part, x);
-        else if (x.mode == kFwdPull) warp_tile<S, kFwdPull>(a, sm, ws, ti, T, 0, x);
-        else warp_tile<S, kBwd>(a, sm, ws, ti, T, 0, x);
+        if (x.mode == kFwdPush) warp_tile<S, kFwdPush, EXT>(a, sm, ws, ti, T, part, x);
+        else if (x.mode == kFwdPull) warp_tile<S, kFwdPull, EXT>(a, sm, ws, ti, T, 0, x);
+        else warp_tile<S, kBwd, EXT>(a, sm, ws, ti, T, 0, x);
         __syncwarp();
         it = it_next;
     }
@@ -747,7 +776,7 @@ __device__ void run_sweep(const BatchArgs &a, Smem<S> &sm, const SweepCtx &x, co
     }
 }
 
-template <int S>
+template <int S, bool EXT>
 __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem<S> &sm = *reinterpret_cast<Smem<S> *>(smem_raw);
@@ -820,7 +849,8 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
                 for (int k = 0; k < S; ++k) {
                     if (sm.roots[k] != (uint32_t)v) continue;
                     w[k >> 1] &= ~(0xFFFFu << ((k & 1) * 16));  // level 0
-                    w[VW + 2 * k] = 1u;                         // sigma 1
+                    w[VW + 2 * k] = EXT ? 0u : 1u;               // sigma 1
+                    w[VW + 2 * k + 1] = EXT ? (uint32_t)(kExtOne >> 32) : 0u;
                 }
                 uint4 *p = reinterpret_cast<uint4 *>(a.rows + v * R);
 #pragma unroll
@@ -850,7 +880,7 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
                 const int k = a.xslot[i];
                 unsigned char *row = row_of<S>(a, r);
                 *lvl_at(row, k) = 0;
-                *val_at<S>(row, k) = 1ull;
+                *val_at<S>(row, k) = EXT ? kExtOne : 1ull;
                 const uint2 ri = a.vinfo[r];
                 atomicAdd(&c->visited[k], 1ull);
                 atomicAdd(&c->wsum[k], 1ull + ri.y);
@@ -904,11 +934,11 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
             if (x.mode == kFwdPull) {
                 walked = uall ? (packed ? a.xtiles[b] : a.ntiles) : ulen;
                 const bool ranged = uall && packed;
-                run_sweep<S>(a, sm, x, uall ? nullptr : a.ulist, ustart, walked, ring,
+                run_sweep<S, EXT>(a, sm, x, uall ? nullptr : a.ulist, ustart, walked, ring,
                              ranged ? a.xrange + a.xrbeg[b] : nullptr, ranged ? a.xrbeg[b + 1] - a.xrbeg[b] : 0u);
             } else {
                 walked = lc;
-                run_sweep<S>(a, sm, x, a.lists + lb, 0, lc, 0xFFFFFFFFull);
+                run_sweep<S, EXT>(a, sm, x, a.lists + lb, 0, lc, 0xFFFFFFFFull);
             }
             __syncthreads();
             if (threadIdx.x == 0) {
@@ -972,7 +1002,7 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
             const uint32_t lc = vload32(a.lcnt + dd);
             if (threadIdx.x == 0) sm.next = 0;
             __syncthreads();
-            run_sweep<S>(a, sm, x, a.lists + lb, 0, lc, 0xFFFFFFFFull);
+            run_sweep<S, EXT>(a, sm, x, a.lists + lb, 0, lc, 0xFFFFFFFFull);
             if (!grid_sync(c, nblk, wait_ns)) return;
             trace(a, b, 3u, (uint32_t)dd, lc, 0);
         }
@@ -1000,34 +1030,34 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
 // Host-side launch helpers.
 // ---------------------------------------------------------------------------
 
-template <int S>
+template <int S, bool EXT>
 static int launch_impl(const BatchArgs &a, cudaStream_t st, int *grid_out) {
     const size_t smem = smem_bytes<S>();
-    cudaError_t e = cudaFuncSetAttribute(bc_sweep_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(bc_sweep_kernel<S, EXT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return set_error(BCG_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
     int dev = 0, nsm = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bc_sweep_kernel<S>, kThreads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bc_sweep_kernel<S, EXT>, kThreads, smem);
     if (e != cudaSuccess) return set_error(BCG_ERR_CUDA, "occupancy query: %s", cudaGetErrorString(e));
     if (per_sm < 1) return set_error(BCG_ERR_CUDA, "sweep kernel cannot be resident (smem %zu)", smem);
     int grid = nsm * per_sm;
     if (grid_out) *grid_out = grid;
     BatchArgs args = a;
     void *params[] = {&args};
-    e = cudaLaunchCooperativeKernel((const void *)bc_sweep_kernel<S>, dim3(grid), dim3(kThreads), params, smem, st);
+    e = cudaLaunchCooperativeKernel((const void *)bc_sweep_kernel<S, EXT>, dim3(grid), dim3(kThreads), params, smem, st);
     if (e != cudaSuccess)
         return set_error(e == cudaErrorNoKernelImageForDevice ? BCG_ERR_NOGPU : BCG_ERR_CUDA,
                          "sweep kernel launch: %s", cudaGetErrorString(e));
     return BCG_OK;
 }
 
-int launch_sweep(int S, const BatchArgs &a, cudaStream_t st, int *grid_out) {
+int launch_sweep(int S, const BatchArgs &a, cudaStream_t st, int *grid_out, bool ext) {
     switch (S) {
-        case 1: return launch_impl<1>(a, st, grid_out);
-        case 3: return launch_impl<3>(a, st, grid_out);
-        case 6: return launch_impl<6>(a, st, grid_out);
+        case 1: return ext ? launch_impl<1, true>(a, st, grid_out) : launch_impl<1, false>(a, st, grid_out);
+        case 3: return ext ? launch_impl<3, true>(a, st, grid_out) : launch_impl<3, false>(a, st, grid_out);
+        case 6: return ext ? launch_impl<6, true>(a, st, grid_out) : launch_impl<6, false>(a, st, grid_out);
         default: return set_error(BCG_ERR_ARG, "batch width %d not in {1,3,6}", S);
     }
 }

@@ -119,6 +119,8 @@ typedef struct bcg_stats {
     uint32_t max_depth;      /* deepest BFS level seen */
     uint32_t batch_width;    /* sources per batch (S) */
     double   kernel_ms;      /* device time of the BC kernels (CUDA events) */
+    uint32_t extended_sigma; /* 1: path counts ran as extended-range numbers */
+    uint32_t reserved;
 } bcg_stats;
 
 /* Number of CUDA devices visible (0 when none); never fails. */
@@ -207,6 +209,24 @@ int bcg_run_weighted(bcg_graph *g, const uint32_t *roots, const double *mult,
 
 /* Forces the sources-per-batch width (1, 3 or 6; 0 = automatic). */
 int bcg_set_batch_width(bcg_graph *g, uint32_t width);
+
+/* How shortest-path counts (sigma) are held.  BCG_SIGMA_AUTO (default):
+ * exact uint64; a run in which a count exceeds 2^64 is redone with
+ * extended-range numbers (16-bit exponent, 49-bit significand, rounded to
+ * nearest: about 2^-49 relative error per add) after restoring the
+ * accumulators, and bcg_stats.extended_sigma reports it.  BCG_SIGMA_EXACT:
+ * overflow fails with BCG_ERR_OVERFLOW (the reference's uint32 counts wrap
+ * silently, bc2d.h:14).  BCG_SIGMA_EXTENDED: always extended.  Graphs such
+ * as large grids need it: their path counts reach 2^4000. */
+#define BCG_SIGMA_AUTO      0
+#define BCG_SIGMA_EXACT     1
+#define BCG_SIGMA_EXTENDED  2
+int bcg_set_sigma_mode(bcg_graph *g, int mode);
+
+/* bcg_single_source in extended mode: sigma_ext[v] is v's path count in the
+ * extended encoding (0 = unreachable or 0; otherwise bits 63..48 hold E,
+ * bits 47..0 f, value (2^48 + f) * 2^(E - 32816)). */
+int bcg_single_source_ext(bcg_graph *g, uint32_t src, int32_t *level, uint64_t *sigma_ext, double *delta);
 
 /* ---------------------------------------------------------------------------
  * Batched form: exact all-sources BC of many independent graphs in one

@@ -35,6 +35,7 @@
  * definition against which the pruned GPU path is checked.
  */
 #include <math.h>
+#include <quadmath.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -224,6 +225,131 @@ int oracle_path_length_sum(uint32_t n, const uint32_t *offs, const uint32_t *adj
         free(lvl); free(queue);
     }
     if (total) *total = sum;
+    return err ? -1 : 0;
+}
+
+/* The same algorithm with sigma and delta held as __float128 (113-bit
+ * significand, exponents to 2^16383): the definition for graphs whose path
+ * counts overflow uint64 and double, such as large grids (counts near
+ * 2^4088 on a 2048 x 2048 grid).  Order of operations as brandes_one. */
+static uint64_t brandes_one_q(uint32_t n, const uint32_t *offs, const uint32_t *adj, uint32_t s, int32_t *lvl,
+                              __float128 *sigma, __float128 *delta, uint32_t *queue, uint32_t *lvl_start,
+                              uint32_t *depth_out) {
+    for (uint32_t v = 0; v < n; ++v) { lvl[v] = -1; sigma[v] = 0; delta[v] = 0; }
+    uint32_t head = 0, tail = 0, nlev = 0;
+    lvl[s] = 0;
+    sigma[s] = 1;
+    queue[tail++] = s;
+    lvl_start[0] = 0;
+    while (head < tail) {
+        uint32_t level_end = tail;
+        int32_t d = lvl[queue[head]];
+        lvl_start[++nlev] = level_end;
+        for (; head < level_end; ++head) {
+            uint32_t c = queue[head];
+            for (uint32_t e = offs[c]; e < offs[c + 1]; ++e) {
+                uint32_t r = adj[e];
+                if (lvl[r] == -1) { lvl[r] = d + 1; queue[tail++] = r; }
+                if (lvl[r] == d + 1) sigma[r] += sigma[c];
+            }
+        }
+    }
+    for (int64_t depth = (int64_t)nlev - 2; depth >= 0; --depth) {
+        for (uint32_t i = lvl_start[depth]; i < lvl_start[depth + 1]; ++i) {
+            uint32_t c = queue[i];
+            __float128 acc = delta[c];
+            for (uint32_t e = offs[c]; e < offs[c + 1]; ++e) {
+                uint32_t r = adj[e];
+                if (lvl[r] == (int32_t)depth + 1) acc += (delta[r] + 1) / sigma[r] * sigma[c];
+            }
+            delta[c] = acc;
+        }
+    }
+    if (depth_out) *depth_out = nlev ? nlev - 1 : 0;
+    return tail;
+}
+
+int oracle_single_source_q(uint32_t n, const uint32_t *offs, const uint32_t *adj, uint32_t src, int32_t *level,
+                           double *sigma_log2, double *delta) {
+    if (src >= n) return -1;
+    uint32_t *queue = (uint32_t *)malloc((size_t)n * sizeof(uint32_t));
+    uint32_t *ls = (uint32_t *)malloc(((size_t)n + 2) * sizeof(uint32_t));
+    int32_t *l = (int32_t *)malloc((size_t)n * sizeof(int32_t));
+    __float128 *sg = (__float128 *)malloc((size_t)n * sizeof(__float128));
+    __float128 *dl = (__float128 *)malloc((size_t)n * sizeof(__float128));
+    int rc = (queue && ls && l && sg && dl) ? 0 : -2;
+    if (!rc) {
+        brandes_one_q(n, offs, adj, src, l, sg, dl, queue, ls, NULL);
+        for (uint32_t v = 0; v < n; ++v) {
+            if (level) level[v] = l[v];
+            if (sigma_log2) sigma_log2[v] = sg[v] > 0 ? (double)log2q(sg[v]) : -INFINITY;
+            if (delta) delta[v] = (double)dl[v];
+        }
+    }
+    free(queue); free(ls); free(l); free(sg); free(dl);
+    return rc;
+}
+
+int oracle_bc_q(uint32_t n, const uint32_t *offs, const uint32_t *adj, const uint32_t *sources, uint64_t nsrc,
+                int nthreads, double *bc, oracle_stats *st) {
+    int nt = nthreads > 0 ? nthreads : 1;
+#ifndef _OPENMP
+    nt = 1;
+#endif
+    __float128 *part = (__float128 *)calloc((size_t)nt * n, sizeof(__float128));
+    if (!part) return -2;
+    uint64_t skipped = 0, visited = 0, teps_edges = 0, ran = 0;
+    uint32_t maxdepth = 0;
+    int err = 0;
+#pragma omp parallel num_threads(nt) reduction(+ : skipped, visited, teps_edges, ran) reduction(max : maxdepth) \
+    reduction(| : err)
+    {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+        int32_t *lvl = (int32_t *)malloc((size_t)n * sizeof(int32_t));
+        __float128 *sigma = (__float128 *)malloc((size_t)n * sizeof(__float128));
+        __float128 *delta = (__float128 *)malloc((size_t)n * sizeof(__float128));
+        uint32_t *queue = (uint32_t *)malloc((size_t)n * sizeof(uint32_t));
+        uint32_t *ls = (uint32_t *)malloc(((size_t)n + 2) * sizeof(uint32_t));
+        __float128 *mine = part + (size_t)tid * n;
+        if (!lvl || !sigma || !delta || !queue || !ls) err = 1;
+#pragma omp for schedule(dynamic, 1)
+        for (int64_t i = 0; i < (int64_t)nsrc; ++i) {
+            if (err) continue;
+            uint32_t s = sources[i];
+            if (s >= n) { err = 1; continue; }
+            if (offs[s + 1] == offs[s]) { skipped++; continue; }
+            uint32_t depth = 0;
+            uint64_t nv = brandes_one_q(n, offs, adj, s, lvl, sigma, delta, queue, ls, &depth);
+            uint64_t degsum = 0;
+            for (uint64_t q = 0; q < nv; ++q) {
+                uint32_t v = queue[q];
+                degsum += offs[v + 1] - offs[v];
+                if (v != s) mine[v] += delta[v];
+            }
+            visited += nv;
+            teps_edges += degsum / 2;
+            ran++;
+            if (depth > maxdepth) maxdepth = depth;
+        }
+        free(lvl); free(sigma); free(delta); free(queue); free(ls);
+    }
+    for (uint32_t v = 0; v < n; ++v) {
+        __float128 acc = 0;
+        for (int t = 0; t < nt; ++t) acc += part[(size_t)t * n + v];
+        bc[v] += (double)acc;
+    }
+    free(part);
+    if (st) {
+        st->skipped = skipped;
+        st->ran = ran;
+        st->visited = visited;
+        st->teps_edges = teps_edges;
+        st->max_depth = maxdepth;
+        st->overflow = 0;
+    }
     return err ? -1 : 0;
 }
 

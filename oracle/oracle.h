@@ -21,5 +21,11 @@ int oracle_bc(uint32_t n, const uint32_t *offs, const uint32_t *adj, const uint3
  * the exact total of bc[] over that source set. */
 int oracle_path_length_sum(uint32_t n, const uint32_t *offs, const uint32_t *adj, const uint32_t *sources,
                            uint64_t nsrc, int nthreads, uint64_t *total);
+/* Sigma and delta as __float128 (graphs whose path counts overflow uint64):
+ * sigma_log2[v] = log2(sigma_v) (-inf for 0). */
+int oracle_single_source_q(uint32_t n, const uint32_t *offs, const uint32_t *adj, uint32_t src, int32_t *level,
+                           double *sigma_log2, double *delta);
+int oracle_bc_q(uint32_t n, const uint32_t *offs, const uint32_t *adj, const uint32_t *sources, uint64_t nsrc,
+                int nthreads, double *bc, oracle_stats *st);
 int oracle_max_threads(void);
 #endif

@@ -47,6 +47,11 @@ def lib():
         L.oracle_bc.argtypes = [ctypes.c_uint32, _u32p, _u32p, _u32p, ctypes.c_uint64, ctypes.c_int, _f64p,
                                 ctypes.POINTER(OracleStats)]
         L.oracle_max_threads.restype = ctypes.c_int
+        L.oracle_single_source_q.restype = ctypes.c_int
+        L.oracle_single_source_q.argtypes = [ctypes.c_uint32, _u32p, _u32p, ctypes.c_uint32, _i32p, _f64p, _f64p]
+        L.oracle_bc_q.restype = ctypes.c_int
+        L.oracle_bc_q.argtypes = [ctypes.c_uint32, _u32p, _u32p, _u32p, ctypes.c_uint64, ctypes.c_int, _f64p,
+                                  ctypes.POINTER(OracleStats)]
         L.oracle_path_length_sum.restype = ctypes.c_int
         L.oracle_path_length_sum.argtypes = [ctypes.c_uint32, _u32p, _u32p, _u32p, ctypes.c_uint64, ctypes.c_int,
                                              _u64p]
@@ -100,6 +105,34 @@ def path_length_sum(offsets, adj, sources, nthreads: int = 1) -> int:
     if rc:
         raise RuntimeError(f"oracle_path_length_sum failed ({rc})")
     return int(tot.value)
+
+
+def single_source_q(offsets, adj, src: int):
+    """__float128 restatement -> (level int32[n], log2 sigma float64[n] (-inf: 0), delta float64[n])."""
+    offsets, adj = _u32(offsets), _u32(adj)
+    n = len(offsets) - 1
+    lvl = np.zeros(n, np.int32)
+    sl = np.zeros(n, np.float64)
+    dl = np.zeros(n, np.float64)
+    rc = lib().oracle_single_source_q(n, offsets.ctypes.data_as(_u32p), adj.ctypes.data_as(_u32p), src,
+                                      lvl.ctypes.data_as(_i32p), sl.ctypes.data_as(_f64p), dl.ctypes.data_as(_f64p))
+    if rc:
+        raise RuntimeError(f"oracle_single_source_q failed ({rc})")
+    return lvl, sl, dl
+
+
+def bc_q(offsets, adj, sources, nthreads: int = 1):
+    """__float128 restatement of bc() for graphs whose path counts overflow uint64."""
+    offsets, adj = _u32(offsets), _u32(adj)
+    s = _u32(sources)
+    n = len(offsets) - 1
+    out = np.zeros(n, np.float64)
+    st = OracleStats()
+    rc = lib().oracle_bc_q(n, offsets.ctypes.data_as(_u32p), adj.ctypes.data_as(_u32p), s.ctypes.data_as(_u32p),
+                           len(s), nthreads, out.ctypes.data_as(_f64p), ctypes.byref(st))
+    if rc:
+        raise RuntimeError(f"oracle_bc_q failed ({rc})")
+    return out, {f: getattr(st, f) for f, _ in st._fields_}
 
 
 def max_threads() -> int:

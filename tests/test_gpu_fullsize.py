@@ -64,3 +64,36 @@ def test_workload_bc_total(big):
         bc = G.bc()
     assert np.all(bc >= -1e-9)
     assert abs(bc.sum() - total) <= 1e-9 * total, (bc.sum(), total)
+
+
+GRID = "grid:w=2048,h=2048,drop=0.05,seed=3"
+
+
+@pytest.fixture(scope="module")
+def grid():
+    offs, adj = bcg.generate(GRID)
+    src = bcg.sample_sources(len(offs) - 1, 256, 3)
+    return offs, adj, src
+
+
+def test_grid_workload_total_and_two_sources(grid):
+    """The 2048 x 2048 grid workload (5% of edges dropped, largest component,
+    256 sources): path counts near 2^4000, so the run switches to extended
+    counts; the bc total must meet the path-length identity and two full
+    single-source runs must match the __float128 oracle."""
+    offs, adj, src = grid
+    total = oracle.path_length_sum(offs, adj, src, nthreads=oracle.max_threads())
+    with bcg.Graph(offs, adj, bcg.PRUNE_DEGREE1) as G:
+        st = G.run(src)
+        bc = G.bc()
+    assert st.extended_sigma == 1 and st.max_depth > 2000
+    assert abs(bc.sum() - total) <= 1e-9 * total, (bc.sum(), total)
+    with bcg.Graph(offs, adj) as G:
+        for s in src[:2]:
+            lvl, slog, dl = G.single_source_ext(int(s))
+            ol, oslog, odl = oracle.single_source_q(offs, adj, int(s))
+            assert np.array_equal(lvl, ol)
+            fin = np.isfinite(oslog)
+            assert np.max(np.abs(slog[fin] - oslog[fin])) < 1e-9
+            assert oslog[fin].max() > 2000
+            assert_bc_close(dl, odl, f"grid delta s={s}")
