@@ -419,6 +419,8 @@ def run_grid(args, rank, world):
     src = bcg.sample_sources(n, 256, 3)
     g = bcg.Graph(offs, adj, bcg.PRUNE_DEGREE1)
     g.set_sigma_mode(bcg.SIGMA_EXTENDED)  # the counts do not fit uint64; no aborted exact attempt is timed
+    if args.width:
+        g.set_batch_width(args.width)
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     for _ in range(max(1, args.warmup)):
         g.reset()
@@ -490,6 +492,7 @@ def main():
     ap.add_argument("--exact-max-scale", type=int, default=16,
                     help="serving form: exact requests on larger graphs are left out (hours each)")
     ap.add_argument("--wave-batches", type=int, default=64, help="serving form: batches per graph per wave")
+    ap.add_argument("--width", type=int, default=0, help="grid form: sources per batch (0: automatic)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -120,7 +120,7 @@ __device__ bool grid_sync(Ctrl *c, unsigned int nblocks, unsigned long long wait
         __threadfence();
     }
     __syncthreads();
-    return *reinterpret_cast<volatile int *>(&c->error) == 0;
+    return *reinterpret_cast<volatile int *>(&c->error) == 0 && *reinterpret_cast<volatile int *>(&c->overflow) == 0;
 }
 
 // ---- state-row field access (row words: levels in halfwords, then values)
@@ -364,12 +364,10 @@ __device__ __forceinline__ void flush_counts(WarpSmem<S> &ws, const LaneCounts<S
     __syncwarp();
 }
 
-// A wrapped uint64 sum: flag it and stop the launch at the next barrier (the
-// host then fails the run or redoes it with extended counts).
-__device__ __forceinline__ void flag_overflow(Ctrl *c) {
-    c->overflow = 1;
-    atomicCAS(&c->error, 0, BCG_ERR_OVERFLOW);
-}
+// A wrapped uint64 sum: flag it (a plain store keeps the unrolled sum sites
+// small); every CTA leaves at the next grid barrier, and the host fails the
+// run or redoes it with extended counts.
+__device__ __forceinline__ void flag_overflow(Ctrl *c) { c->overflow = 1; }
 
 // Value arithmetic of a sweep.  Forward sweeps sum sigma values, backward
 // sweeps sum X = (1 + delta) / sigma values; with EXT both are extended-range
