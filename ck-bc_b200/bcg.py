@@ -29,6 +29,7 @@ ERR_NOGPU = -9
 
 PRUNE_DEGREE1 = 0x1
 DIRECTED = 0x2
+PRUNE_TREES = 0x4
 
 SIGMA_AUTO = 0
 SIGMA_EXACT = 1

@@ -190,6 +190,7 @@ static void graph_free(bcg_graph *g) {
     cudaFree(g->d_tiles); cudaFree(g->d_hub_acc); cudaFree(g->d_hub_cnt);
     cudaFree(g->d_tile_of); cudaFree(g->d_tmark); cudaFree(g->d_lists);
     cudaFree(g->d_lbase); cudaFree(g->d_lcnt); cudaFree(g->d_ulist); cudaFree(g->d_bc_save);
+    cudaFree(g->d_tree_acc);
     cudaFree(g->d_rows); cudaFree(g->d_ctrl);
     cudaFree(g->d_roots); cudaFree(g->d_pend); cudaFree(g->d_mult); cudaFree(g->d_rstat);
     if (g->ev0) cudaEventDestroy(g->ev0);
@@ -347,7 +348,34 @@ struct RunPlan {
     std::vector<double> mult;
     std::vector<uint64_t> count;  // sources mapped to each root
     uint64_t skipped = 0;
+    // trees mode: sources in components that are trees (no search needed)
+    uint64_t tree_only = 0, tree_edges = 0, tree_verts = 0;
 };
+
+__global__ void k_add(uint32_t n, double *__restrict__ bc, const double *__restrict__ x) {
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < n) bc[v] += x[v];
+}
+
+// Trees mode: the closed-form bc of the tree vertices (and the anchors' tree
+// terms) for this run's sources, added on the device after the search.
+static int add_tree_terms(bcg_graph *g, const uint32_t *src, uint64_t nsrc, const RunPlan &p, cudaStream_t st,
+                          bcg_stats *stats) {
+    std::vector<uint32_t> cnt(g->n, 0);
+    for (uint64_t i = 0; i < nsrc; ++i)
+        if (g->h_deg[src[i]]) ++cnt[src[i]];
+    std::vector<double> acc;
+    tree_bc(g->tinfo, cnt, acc);
+    CK(cudaMemcpyAsync(g->d_tree_acc, acc.data(), (size_t)g->n * sizeof(double), cudaMemcpyHostToDevice, st));
+    k_add<<<(g->n + 255) / 256, 256, 0, st>>>(g->n, g->d_bc, g->d_tree_acc);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
+    if (stats) {
+        stats->teps_edges += p.tree_edges;
+        stats->comp_vertices += p.tree_verts;
+    }
+    return BCG_OK;
+}
 
 static int plan_run(const bcg_graph *g, const uint32_t *src, uint64_t nsrc, RunPlan &p) {
     std::unordered_map<uint32_t, uint32_t> idx;
@@ -357,6 +385,13 @@ static int plan_run(const bcg_graph *g, const uint32_t *src, uint64_t nsrc, RunP
         if (s >= g->n) return set_error(BCG_ERR_ARG, "source %u >= n=%u", s, g->n);
         if (g->h_deg[s] == 0) { ++p.skipped; continue; }
         const uint32_t r = g->h_anchor.empty() ? s : g->h_anchor[s];
+        if (g->trees && g->h_cdeg[r] == 0) {
+            // a tree component: no kept edges, its bc is all in the tree terms
+            ++p.tree_only;
+            p.tree_edges += g->tinfo.comp_n[g->tinfo.comp[s]] - 1;
+            p.tree_verts += g->tinfo.comp_n[g->tinfo.comp[s]];
+            continue;
+        }
         auto it = idx.find(r);
         uint32_t k;
         if (it == idx.end()) {
@@ -371,7 +406,7 @@ static int plan_run(const bcg_graph *g, const uint32_t *src, uint64_t nsrc, RunP
         }
         p.mult[k] += 1.0;
         p.count[k] += 1;
-        if (r != s) p.pend[k] += 1;
+        if (r != s && !g->trees) p.pend[k] += 1;
     }
     return BCG_OK;
 }
@@ -638,10 +673,33 @@ static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint3
         rc = validate_csr(offsets, adj, n, nnz);
         if (rc) return rc;
     }
+    // iterated pendant-tree pruning: the device holds the kept graph only
+    const bool trees = (flags & BCG_PRUNE_TREES) && !(flags & BCG_DIRECTED);
+    bcg::TreeInfo tinfo;
+    std::vector<uint32_t> core_offs, core_adj, h_adj_copy;
+    const uint32_t *orig_offs = ho;
+    if (trees) {
+        const uint32_t *hadj = adj;
+        if (device_in) {
+            h_adj_copy.resize(nnz);
+            if (nnz && cudaMemcpy(h_adj_copy.data(), adj, nnz * sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+                return set_error(BCG_ERR_CUDA, "reading adjacency");
+            for (uint64_t e = 0; e < nnz; ++e)
+                if (h_adj_copy[e] >= n) return set_error(BCG_ERR_ARG, "adj[%" PRIu64 "] = %u >= n", e, h_adj_copy[e]);
+            hadj = h_adj_copy.data();
+        }
+        peel_trees(ho, hadj, n, tinfo, core_offs, core_adj);
+        offsets = core_offs.data();
+        adj = core_adj.data();
+        ho = core_offs.data();
+        device_in = false;
+        flags &= ~BCG_PRUNE_DEGREE1;
+    }
+    const uint64_t dev_nnz = trees ? core_adj.size() : nnz;
     bcg_graph *g = new bcg_graph();
     cudaGetDevice(&g->device);
     g->n = n;
-    g->nnz = nnz;
+    g->nnz = dev_nnz;
     g->flags = flags;
     if (const char *e = getenv("BCG_PUSH_PULL_RATIO")) g->ratio = (float)atof(e);
     auto fail = [&](int code) { graph_free(g); return code; };
@@ -649,15 +707,32 @@ static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint3
     if ((e = cudaMalloc(&g->d_offs, ((size_t)n + 1) * sizeof(uint32_t))) != cudaSuccess ||
         // 4 entries of tail padding: the sweep copies adjacency ranges in
         // 16-byte aligned chunks that may end up to 12 bytes past nnz
-        (e = cudaMalloc(&g->d_adj, (nnz + 4) * sizeof(uint32_t))) != cudaSuccess)
+        (e = cudaMalloc(&g->d_adj, (dev_nnz + 4) * sizeof(uint32_t))) != cudaSuccess)
         return fail(set_error(BCG_ERR_OOM, "cudaMalloc CSR: %s", cudaGetErrorString(e)));
     const cudaMemcpyKind kind = device_in ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     if ((e = cudaMemcpy(g->d_offs, offsets, ((size_t)n + 1) * sizeof(uint32_t), kind)) != cudaSuccess ||
-        (nnz && (e = cudaMemcpy(g->d_adj, adj, nnz * sizeof(uint32_t), kind)) != cudaSuccess) ||
-        (e = cudaMemset(g->d_adj + nnz, 0, 4 * sizeof(uint32_t))) != cudaSuccess)
+        (dev_nnz && (e = cudaMemcpy(g->d_adj, adj, dev_nnz * sizeof(uint32_t), kind)) != cudaSuccess) ||
+        (e = cudaMemset(g->d_adj + dev_nnz, 0, 4 * sizeof(uint32_t))) != cudaSuccess)
         return fail(set_error(BCG_ERR_CUDA, "uploading CSR: %s", cudaGetErrorString(e)));
     rc = create_common(g, ho);
     if (rc) return fail(rc);
+    if (trees) {
+        // kept-graph degrees for the searches, input degrees for the source
+        // skip test, and every kept vertex weighted by its trees (reach)
+        g->trees = true;
+        g->nnz = nnz;
+        g->h_cdeg = g->h_deg;
+        for (uint32_t v = 0; v < n; ++v) g->h_deg[v] = orig_offs[v + 1] - orig_offs[v];
+        g->tinfo = std::move(tinfo);
+        g->h_anchor = g->tinfo.anchor;
+        g->npruned = (uint32_t)g->tinfo.order.size();
+        std::vector<uint2> vi(n);
+        for (uint32_t v = 0; v < n; ++v)
+            vi[v] = make_uint2(g->h_cdeg[v], g->tinfo.parent[v] == kNoRoot ? g->tinfo.sz[v] - 1 : 0u);
+        if ((e = cudaMemcpy(g->d_vinfo, vi.data(), (size_t)n * sizeof(uint2), cudaMemcpyHostToDevice)) != cudaSuccess ||
+            (e = cudaMalloc(&g->d_tree_acc, (size_t)n * sizeof(double))) != cudaSuccess)
+            return fail(set_error(BCG_ERR_CUDA, "tree weights: %s", cudaGetErrorString(e)));
+    }
     *out = g;
     return BCG_OK;
 }
@@ -696,7 +771,9 @@ int bcg_run(bcg_graph *g, const uint32_t *sources, uint64_t nsrc, bcg_stats *sta
     RunPlan p;
     int rc = plan_run(g, sources, nsrc, p);
     if (rc) return rc;
-    return run_plan(g, p, 0, st, false, nullptr, nullptr);
+    rc = run_plan(g, p, 0, st, false, nullptr, nullptr);
+    if (rc || !g->trees) return rc;
+    return add_tree_terms(g, sources, nsrc, p, 0, st);
 }
 
 int bcg_run_device(bcg_graph *g, const uint32_t *d_sources, uint64_t nsrc, void *stream, bcg_stats *stats) {
@@ -712,7 +789,9 @@ int bcg_run_device(bcg_graph *g, const uint32_t *d_sources, uint64_t nsrc, void 
     RunPlan p;
     int rc = plan_run(g, h.data(), nsrc, p);
     if (rc) return rc;
-    return run_plan(g, p, st, stats, false, nullptr, nullptr);
+    rc = run_plan(g, p, st, stats, false, nullptr, nullptr);
+    if (rc || !g->trees) return rc;
+    return add_tree_terms(g, h.data(), nsrc, p, st, stats);
 }
 
 int bcg_get_bc(bcg_graph *g, double *bc_host) {
@@ -743,6 +822,7 @@ int bcg_bc_csr(const uint32_t *offsets, const uint32_t *adj, uint32_t n, uint64_
 }
 
 static int single_source_impl(bcg_graph *g, uint32_t src, int32_t *level, uint64_t *sigma, double *delta) {
+    if (g->trees) return set_error(BCG_ERR_ARG, "single-source runs are not available with BCG_PRUNE_TREES");
     clear_error();
     if (!g) return set_error(BCG_ERR_ARG, "null handle");
     if (src >= g->n) return set_error(BCG_ERR_ARG, "source %u >= n=%u", src, g->n);
@@ -842,6 +922,7 @@ int bcg_graph_info(bcg_graph *g, uint32_t *n, uint64_t *nnz, uint64_t *nnz_prune
 int bcg_graph_set_reach(bcg_graph *g, const uint32_t *reach) {
     clear_error();
     if (!g || !reach) return set_error(BCG_ERR_ARG, "null argument");
+    if (g->trees) return set_error(BCG_ERR_ARG, "graph was created with BCG_PRUNE_TREES");
     if (g->flags & BCG_PRUNE_DEGREE1) return set_error(BCG_ERR_ARG, "graph was created with BCG_PRUNE_DEGREE1");
     const size_t n = g->n;
     std::vector<uint2> vi(n);
@@ -854,6 +935,7 @@ int bcg_run_weighted(bcg_graph *g, const uint32_t *roots, const double *mult, co
                      uint64_t nroots, bcg_stats *stats) {
     clear_error();
     if (!g || (nroots && (!roots || !mult))) return set_error(BCG_ERR_ARG, "null argument");
+    if (g->trees) return set_error(BCG_ERR_ARG, "graph was created with BCG_PRUNE_TREES");
     bcg_stats local{};
     bcg_stats *st = stats ? stats : &local;
     *st = bcg_stats{};

@@ -8,11 +8,24 @@
 #include "engine.cuh"
 
 using bcg::Ctrl;
+using bcg::kNoRoot;
 using bcg::RootStat;
 using bcg::Tile;
 using bcg::kDefaultWaitNs;
 using bcg::kTileEdges;
 using bcg::kTileVerts;
+
+namespace bcg {
+// Pendant trees of a graph (BCG_PRUNE_TREES; trees.cpp).
+struct TreeInfo {
+    std::vector<uint32_t> parent;  // vertex it hung from when peeled; kNoRoot for kept (core) vertices
+    std::vector<uint32_t> order;   // peeled vertices, in peeling order (children before parents)
+    std::vector<uint32_t> sz;      // vertices in the subtree (a kept vertex: 1 + its trees)
+    std::vector<uint32_t> anchor;  // the kept vertex a vertex's tree hangs from (itself if kept)
+    std::vector<uint32_t> comp;    // connected component of the input graph
+    std::vector<uint64_t> comp_n;  // vertices per component
+};
+}  // namespace bcg
 
 struct bcg_graph {
     int device = 0;
@@ -45,6 +58,10 @@ struct bcg_graph {
     uint32_t tile_vcap = kTileVerts, tile_ecap = kTileEdges;  // tile shape (autotuned by batches)
     std::vector<uint32_t> tile_breaks;  // sorted vertices where a new tile must start
     float ratio = 0.2f;
+    bool trees = false;               // BCG_PRUNE_TREES: pendant trees folded (tinfo)
+    bcg::TreeInfo tinfo;
+    std::vector<uint32_t> h_cdeg;     // degrees in the kept graph (trees mode)
+    double *d_tree_acc = nullptr;     // tree vertices' closed-form bc of one run
     int sigma_mode = 0;               // 0 auto (exact, extended on overflow), 1 exact only, 2 extended
     double *d_bc_save = nullptr;      // accumulators before an automatic-mode run
     unsigned long long wait_ns = kDefaultWaitNs;
@@ -76,6 +93,12 @@ int enqueue_packed(bcg_graph *g, const PackedRun &p, uint32_t S, cudaStream_t st
 int check_ctrl(bcg_graph *g, cudaStream_t st);
 // Rebuilds the work tiles with another shape (vcap vertices, ecap entries).
 int graph_retile(bcg_graph *g, uint32_t vcap, uint32_t ecap, bool force = false);
+// Peels every pendant tree off the graph (t) and returns the kept graph's CSR.
+void peel_trees(const uint32_t *offs, const uint32_t *adj, uint32_t n, TreeInfo &t,
+                std::vector<uint32_t> &core_offs, std::vector<uint32_t> &core_adj);
+// Closed-form bc of the tree vertices (and the anchors' tree terms) for the
+// source multiplicities cnt[v].
+void tree_bc(const TreeInfo &t, const std::vector<uint32_t> &cnt, std::vector<double> &acc);
 // Uploads ngraphs host CSR graphs as one disjoint union (graph order[p] at
 // union position p, its vertex v at base[order[p]] + v; with by_active the
 // graphs with most non-isolated vertices come first).  hdeg: union degrees.

@@ -46,6 +46,11 @@ extern "C" {
 #define BCG_PRUNE_DEGREE1   0x1u  /* fold degree-1 vertices into their neighbour (bc2d -H 1) */
 #define BCG_DIRECTED        0x2u  /* adjacency is not symmetric (bc2d -U): traversal follows
                                      adj[] only; pruning is ignored */
+#define BCG_PRUNE_TREES     0x4u  /* fold whole pendant trees (iterated degree-1 removal), not
+                                     just one layer as degree_reduction does (bc2d.c:314-419);
+                                     the trees' betweenness is computed in closed form.  Takes
+                                     precedence over BCG_PRUNE_DEGREE1.  Not available with
+                                     bcg_single_source, bcg_graph_set_reach, bcg_run_weighted. */
 
 /* ---------------------------------------------------------------------------
  * Host-side graph ingest and generation (host code, no GPU needed).

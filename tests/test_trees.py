@@ -1,0 +1,90 @@
+"""Iterated pendant-tree pruning, host part (CPU only).
+
+ck-bc_b200/csrc/trees.cpp is compiled into a small harness.  On a forest
+every vertex is peeled (or is the last vertex of its tree), no core search
+runs, and the closed-form tree terms must equal the oracle's Brandes bc for
+any source multiset."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import bcg
+import oracle
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+HARNESS = r"""
+#include <cstdio>
+#include <vector>
+#include "engine_internal.hpp"
+using namespace bcg;
+int main() {
+    unsigned n, m, k;
+    if (scanf("%u %u %u", &n, &m, &k) != 3) return 1;
+    std::vector<uint32_t> offs(n + 1), adj(m), cnt(n, 0);
+    for (auto &x : offs) scanf("%u", &x);
+    for (auto &x : adj) scanf("%u", &x);
+    for (unsigned i = 0; i < k; ++i) { unsigned s; scanf("%u", &s); if (offs[s + 1] > offs[s]) ++cnt[s]; }
+    TreeInfo t;
+    std::vector<uint32_t> co, ca;
+    peel_trees(offs.data(), adj.data(), n, t, co, ca);
+    std::vector<double> acc;
+    tree_bc(t, cnt, acc);
+    printf("%zu %zu\n", t.order.size(), ca.size());
+    for (unsigned v = 0; v < n; ++v) printf("%.17g %u\n", acc[v], t.anchor[v]);
+}
+"""
+
+
+@pytest.fixture(scope="module")
+def harness(tmp_path_factory):
+    d = tmp_path_factory.mktemp("trees")
+    (d / "h.cpp").write_text(HARNESS)
+    exe = d / "h"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "ck-bc_b200", "csrc"), "-I",
+                    os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include",
+                    os.path.join(ROOT, "ck-bc_b200", "csrc", "trees.cpp"), str(d / "h.cpp"), "-o", str(exe)],
+                   check=True)
+
+    def run(offs, adj, src):
+        n = len(offs) - 1
+        txt = f"{n} {len(adj)} {len(src)}\n" + " ".join(map(str, offs)) + "\n" + " ".join(map(str, adj)) + "\n"
+        txt += " ".join(map(str, src)) + "\n"
+        out = subprocess.run([str(exe)], input=txt, capture_output=True, text=True, check=True).stdout.split("\n")
+        peeled, core_nnz = map(int, out[0].split())
+        vals = [line.split() for line in out[1:1 + n]]
+        return peeled, core_nnz, np.array([float(a) for a, _ in vals]), np.array([int(b) for _, b in vals])
+
+    return run
+
+
+def _forest(rng, sizes):
+    pairs, base = [], 0
+    for k in sizes:
+        for i in range(1, k):
+            pairs.append((base + i, base + int(rng.integers(0, i))))  # random recursive tree
+        base += k
+    return bcg.from_pairs(np.array(pairs, dtype=np.uint64).reshape(-1, 2), base)
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_forest_tree_terms_equal_brandes(harness, seed):
+    rng = np.random.default_rng(seed)
+    offs, adj = _forest(rng, [1, 2, 3, 7, 20, 41])
+    n = len(offs) - 1
+    for src in (np.arange(n), rng.integers(0, n, size=30), np.array([5, 5, 5, 10])):
+        peeled, core_nnz, acc, _ = harness(offs, adj, src)
+        ref, _ = oracle.bc(offs, adj, np.asarray(src, dtype=np.uint32))
+        assert core_nnz == 0
+        np.testing.assert_allclose(acc, ref, rtol=1e-12, atol=1e-9)
+
+
+def test_peeling_anchors_and_core(harness):
+    # triangle 0-1-2 with a path 2-3-4 and a star 1-5,1-6, plus an isolated edge 7-8
+    offs, adj = bcg.from_pairs([[0, 1], [1, 2], [2, 0], [2, 3], [3, 4], [1, 5], [1, 6], [7, 8]], 9)
+    peeled, core_nnz, acc, anchor = harness(offs, adj, [])
+    assert core_nnz == 6 and peeled == 5  # 3, 4, 5, 6 and one end of the isolated edge
+    assert anchor.tolist()[:7] == [0, 1, 2, 2, 2, 1, 1]
+    assert anchor[7] == anchor[8] and anchor[7] in (7, 8)
