@@ -3,7 +3,8 @@
 Workload (N=1): R-MAT scale 20, edge factor 16, (a,b,c,d) = (0.57,0.19,0.19,
 0.05), seed 2, plus pendant trees on 10% of the vertices (Geometric sizes,
 mean 4); 4096 sources drawn uniformly without replacement with seed 2;
-degree-1 pruning on; FP64 delta/bc, uint64 sigma.  Seeded synthetic input:
+pendant-tree pruning on (--prune degree1: one layer, as bc2d -H 1); FP64
+delta/bc, uint64 sigma.  Seeded synthetic input:
 no public dataset is involved.
 
 A step = one exact-BC pass over the step's sources (one kernel launch of the
@@ -119,13 +120,17 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def traffic_per_source():
-    """DRAM bytes per source of the sweep kernel from the committed ncu summary."""
+def traffic_per_source(prune: str):
+    """DRAM bytes per root of the sweep kernel from the committed ncu summary
+    of the same pruning mode (profiles/sweep_traffic.json), else None."""
     p = os.path.join(ROOT, "profiles", "sweep_traffic.json")
     try:
         with open(p) as f:
             d = json.load(f)
-        return float(d["dram_bytes_per_source"]), d.get("note", "")
+        e = d[prune] if prune in d else (d if prune == "degree1" and "dram_bytes_per_source" in d else None)
+        if e is None:
+            return None, ""
+        return float(e["dram_bytes_per_source"]), e.get("note", "")
     except Exception:
         return None, ""
 
@@ -417,7 +422,8 @@ def run_grid(args, rank, world):
     offs, adj = bcg.generate(spec)
     n = len(offs) - 1
     src = bcg.sample_sources(n, 256, 3)
-    g = bcg.Graph(offs, adj, bcg.PRUNE_DEGREE1)
+    pflag = bcg.PRUNE_TREES if args.prune == "trees" else bcg.PRUNE_DEGREE1
+    g = bcg.Graph(offs, adj, pflag)
     g.set_sigma_mode(bcg.SIGMA_EXTENDED)  # the counts do not fit uint64; no aborted exact attempt is timed
     if args.width:
         g.set_batch_width(args.width)
@@ -439,7 +445,7 @@ def run_grid(args, rank, world):
     kern_s = sum(ms) / len(ms) / 1e3
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    with bcg.Graph(offs, adj, bcg.PRUNE_DEGREE1) as ge:
+    with bcg.Graph(offs, adj, pflag) as ge:
         ste = ge.run(src)
         ge.bc()
     e2e_s = time.perf_counter() - t0
@@ -493,6 +499,9 @@ def main():
                     help="serving form: exact requests on larger graphs are left out (hours each)")
     ap.add_argument("--wave-batches", type=int, default=64, help="serving form: batches per graph per wave")
     ap.add_argument("--width", type=int, default=0, help="grid form: sources per batch (0: automatic)")
+    ap.add_argument("--prune", default="trees", choices=["degree1", "trees"],
+                    help="plain/grid forms: whole pendant trees (default) or one layer of degree-1 vertices "
+                         "(as bc2d -H 1)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -534,7 +543,8 @@ def main():
     srcs = np.ascontiguousarray(all_src[rank * ns:(rank + 1) * ns])
     log(f"[rank {rank}] graph n={n} nnz={len(adj)} generated in {time.perf_counter() - t_gen:.1f}s")
 
-    g = bcg.Graph(offs, adj, bcg.PRUNE_DEGREE1)
+    pflag = bcg.PRUNE_TREES if args.prune == "trees" else bcg.PRUNE_DEGREE1
+    g = bcg.Graph(offs, adj, pflag)
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     bc_t = torch.as_tensor(bcg.DeviceArray(g.bc_device_ptr(), n), device="cuda")
     stream = torch.cuda.current_stream()
@@ -584,7 +594,7 @@ def main():
     alg_bytes = 16.0 * edges + 56.0 * cverts + 8.0 * ran
     kern_s = sum(kern_ms) / 1e3
     achieved = alg_bytes / kern_s / 1e9
-    tps, tnote = traffic_per_source()
+    tps, tnote = traffic_per_source(args.prune)
     traffic = tps * (ran / args.steps) if tps is not None else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": peak_kind, "traffic": traffic,
@@ -602,7 +612,7 @@ def main():
     for _ in range(e2e_steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        ge = bcg.Graph(h_offs, h_adj, bcg.PRUNE_DEGREE1)
+        ge = bcg.Graph(h_offs, h_adj, pflag)
         st = ge.run(srcs)
         if dist is not None:
             bt = torch.as_tensor(bcg.DeviceArray(ge.bc_device_ptr(), n), device="cuda")
@@ -633,7 +643,8 @@ def main():
                "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                "config": {"workload": WORKLOAD, "graph": SPEC, "n": n, "m": len(adj) // 2,
-                          "sources_per_gpu": ns, "source_seed": SRC_SEED, "pruning": "degree-1",
+                          "sources_per_gpu": ns, "source_seed": SRC_SEED,
+                          "pruning": "pendant trees" if args.prune == "trees" else "degree-1",
                           "sources_skipped_per_step": int(st.skipped), "batch_width": int(st.batch_width),
                           "parallelism": f"source-sharded x{world}" if world > 1 else "1 GPU",
                           "l2": "512 MiB flush write between steps (untimed); graph + state exceed L2"},
