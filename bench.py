@@ -408,7 +408,7 @@ def run_serve(args, rank, world):
 def run_grid(args, rank, world):
     """High-diameter workload: 2048 x 2048 grid, each edge dropped with
     probability 0.05 (seed 3), largest component kept; 256 sources (seed 3),
-    degree-1 pruning.  Path counts reach about 2^4000, so the run switches to
+    pendant-tree pruning (--prune degree1: one layer).  Path counts reach about 2^4000, so the run switches to
     extended-range counts (bcg_stats.extended_sigma).  value: TEPS over the
     device time of the run; cpu_baseline: the oracle's __float128 restatement
     on a bounded sample of the sources.  One GPU (replicas only)."""
@@ -466,7 +466,7 @@ def run_grid(args, rank, world):
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "ext64", "data": "synthetic",
            "impl": "bcg-grid",
            "config": {"workload": "grid2048_drop5_256src", "graph": spec, "n": n, "m": len(adj) // 2,
-                      "sources": 256, "source_seed": 3, "pruning": "degree-1",
+                      "sources": 256, "source_seed": 3, "pruning": "pendant trees" if args.prune == "trees" else "degree-1",
                       "sigma": "extended (set explicitly)", "extended_sigma": int(st.extended_sigma),
                       "max_depth": int(st.max_depth),
                       "batch_width": int(st.batch_width),
