@@ -21,7 +21,9 @@
 // Extensions (letters unused by the reference): -s <file> source list (one id
 // per line), -F full-precision output ("%.17g" of bc/2), -G <spec> generator
 // spec (see bcg_csr_generate), -W <1|3|6> sources per batch, -B <path> binary
-// CSR cache of the -f graph (read when it exists, else written after parsing).
+// CSR cache of the -f graph (read when it exists, else written after parsing),
+// -T fold whole pendant trees instead of one degree-1 layer (implies -H 1;
+// BCG_PRUNE_TREES).
 #include <getopt.h>
 #include <sys/time.h>
 
@@ -68,6 +70,7 @@ static double now_us() {
            "\t\t -G <spec> generate a graph (rmat:/er:/grid: spec)\n"
            "\t\t -B <path> binary CSR cache of the -f graph (read if present, else written)\n"
            "\t\t -W <1|3|6> sources per batch\n"
+           "\t\t -T fold whole pendant trees (iterated 1-degree reduction; implies -H 1)\n"
            "\n",
            pname);
 }
@@ -80,7 +83,7 @@ int main(int argc, char *argv[]) {
     if (argc == 1) usage(argv[0]);
     int gread = -1;
     int scale = 21, edgef = 16;
-    int debug = 0, heuristic = 0, undirected = 1, random_root = 0, mono = 1, full = 0;
+    int debug = 0, heuristic = 0, undirected = 1, random_root = 0, mono = 1, full = 0, trees = 0;
     int R = 0, C = 0, rootset = 0;
     uint32_t width = 0;
     uint64_t N = 0, startv = 0;
@@ -92,7 +95,7 @@ int main(int argc, char *argv[]) {
     fprintf(stdout, "%s\n\n", cmdline.c_str());
 
     int opt;
-    while ((opt = getopt(argc, argv, "o:p:amhDR:Uf:n:r:S:E:N:H:s:FG:W:B:")) != EOF) {
+    while ((opt = getopt(argc, argv, "o:p:amhDR:Uf:n:r:S:E:N:H:s:FG:W:B:T")) != EOF) {
 #define CHECKRTYPE(exitval, o)                                        \
     {                                                                 \
         if ((exitval) == gread) prexit("Unexpected option -%c!\n", o); \
@@ -102,6 +105,7 @@ int main(int argc, char *argv[]) {
             case 'H':
                 if (0 == sscanf(optarg, "%d", &heuristic)) prexit("Invalid Heuristic Option (-H): %s\n", optarg);
                 break;
+            case 'T': trees = 1; break;
             case 'o': ofile = optarg; break;
             case 'p': {
                 char buf[64];
@@ -174,6 +178,7 @@ int main(int argc, char *argv[]) {
         if (!outdebug) prexit("Cannot open file %s...\n", "debug_0.log");
     }
     if (rootset > 0) random_root = 0;
+    if (trees && heuristic == 0) heuristic = 1;
 
     fprintf(stdout, "\n\n****** DEVEL VERSION ******\n\n\n\n***************************\n\n");
     fprintf(stdout, "Total number of vertices (N): %" PRIu64 "\n", N);
@@ -190,7 +195,7 @@ int main(int argc, char *argv[]) {
     }
     fprintf(stdout, "\n\n");
     if (heuristic == 0) fprintf(stdout, "HEURISTICs: OFF: %d\n", heuristic);
-    else if (heuristic == 1) fprintf(stdout, "HEURISTICs: 1-degree reduction ON: %d\n", heuristic);
+    else if (heuristic == 1) fprintf(stdout, "HEURISTICs: 1-degree reduction ON: %d%s\n", heuristic, trees ? " (whole pendant trees)" : "");
     fprintf(stdout, "PREFIX SCAN library: none (device-side level loop)\n");
     fprintf(stdout, "OVERLAP: ON\n");
     fprintf(stdout, "PREFIX SCAN optimization: ON\n");
@@ -258,7 +263,7 @@ int main(int argc, char *argv[]) {
     }
 
     uint32_t flags = 0;
-    if (heuristic == 1) flags |= BCG_PRUNE_DEGREE1;
+    if (heuristic == 1) flags |= trees ? BCG_PRUNE_TREES : BCG_PRUNE_DEGREE1;
     if (!undirected) flags |= BCG_DIRECTED;
     bcg_graph *dg = nullptr;
     double tr0 = now_us();

@@ -38,13 +38,14 @@ def graph_file(tmp_path_factory):
     return p, offs, adj
 
 
-@pytest.mark.parametrize("heur", [0, 1])
+@pytest.mark.parametrize("heur", ["0", "1", "1T"])
 def test_cli_range_full_precision(graph_file, tmp_path, heur):
     path, offs, adj = graph_file
     n = len(offs) - 1
     out = str(tmp_path / "res")
-    r = subprocess.run([BC2D, "-p", "1x1", "-f", path, "-n", str(n), "-r", "5", "-N", "300", "-H", str(heur),
-                        "-o", out, "-F"], capture_output=True, text=True, timeout=300)
+    extra = ["-T"] if heur.endswith("T") else []
+    r = subprocess.run([BC2D, "-p", "1x1", "-f", path, "-n", str(n), "-r", "5", "-N", "300", "-H", heur[0],
+                        "-o", out, "-F"] + extra, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     assert "BC rounds" in r.stdout and "RESULTS" in r.stdout
     rowpp, ids, vals = _read_result(out + "_1X1_0.log")
