@@ -498,7 +498,7 @@ def main():
     ap.add_argument("--exact-max-scale", type=int, default=16,
                     help="serving form: exact requests on larger graphs are left out (hours each)")
     ap.add_argument("--wave-batches", type=int, default=64, help="serving form: batches per graph per wave")
-    ap.add_argument("--width", type=int, default=0, help="grid form: sources per batch (0: automatic)")
+    ap.add_argument("--width", type=int, default=0, help="sources per batch, 1, 3 or 6 (0: automatic)")
     ap.add_argument("--prune", default="trees", choices=["degree1", "trees"],
                     help="plain/grid forms: whole pendant trees (default) or one layer of degree-1 vertices "
                          "(as bc2d -H 1)")
@@ -545,6 +545,8 @@ def main():
 
     pflag = bcg.PRUNE_TREES if args.prune == "trees" else bcg.PRUNE_DEGREE1
     g = bcg.Graph(offs, adj, pflag)
+    if args.width:
+        g.set_batch_width(args.width)
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     bc_t = torch.as_tensor(bcg.DeviceArray(g.bc_device_ptr(), n), device="cuda")
     stream = torch.cuda.current_stream()
@@ -613,6 +615,8 @@ def main():
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         ge = bcg.Graph(h_offs, h_adj, pflag)
+        if args.width:
+            ge.set_batch_width(args.width)
         st = ge.run(srcs)
         if dist is not None:
             bt = torch.as_tensor(bcg.DeviceArray(ge.bc_device_ptr(), n), device="cuda")

@@ -371,7 +371,7 @@ int bcg_batch_autotune(bcg_batch *b, uint32_t sample_batches, uint32_t *width, u
     clear_error();
     if (!b) return set_error(BCG_ERR_ARG, "null handle");
     static const uint32_t widths[] = {1, 3, 6};
-    static const uint32_t shapes[][2] = {{32, 256}, {32, 128}, {16, 128}, {16, 64}};
+    static const uint32_t shapes[][2] = {{32, 512}, {32, 256}, {32, 128}, {16, 128}, {16, 64}};
     double best = 0.0;
     uint32_t bw = b->width, bv = b->g->tile_vcap, be = b->g->tile_ecap;
     for (const auto &sh : shapes) {

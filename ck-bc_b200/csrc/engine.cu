@@ -28,6 +28,7 @@
 // cuda_kernels.cu:274, 1095).
 #include <algorithm>
 #include <cinttypes>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <unordered_map>
@@ -123,7 +124,8 @@ __global__ void k_levels_out(uint32_t n, const unsigned char *__restrict__ rows,
 
 // Runs of at most vcap consecutive vertices with at most ecap adjacency
 // entries; a vertex with more than ecap entries is split into ecap-entry
-// chunks (vcap <= 32, ecap <= 256: the sweep kernel's lane and run limits).
+// chunks (vcap <= 32, ecap <= kTileEdges: the sweep kernel's lane and
+// staging limits).
 // A tile never spans a vertex listed in `breaks` (sorted) and the vertex
 // before it.  tile_of[v] = index of v's tile (of its first chunk, with
 // kHubFlag, when v is split).
@@ -702,6 +704,14 @@ static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint3
     g->nnz = dev_nnz;
     g->flags = flags;
     if (const char *e = getenv("BCG_PUSH_PULL_RATIO")) g->ratio = (float)atof(e);
+    if (const char *e = getenv("BCG_TILE_SHAPE")) {  // "<vertices>x<entries>", e.g. 32x128
+        unsigned tv = 0, te = 0;
+        if (sscanf(e, "%ux%u", &tv, &te) == 2 && tv >= 1 && tv <= (unsigned)kTileVerts && te >= 1 &&
+            te <= (unsigned)kTileEdges) {
+            g->tile_vcap = tv;
+            g->tile_ecap = te;
+        }
+    }
     auto fail = [&](int code) { graph_free(g); return code; };
     cudaError_t e;
     if ((e = cudaMalloc(&g->d_offs, ((size_t)n + 1) * sizeof(uint32_t))) != cudaSuccess ||

@@ -10,13 +10,18 @@ namespace bcg {
 #define BCG_THREADS 512
 #endif
 #ifndef BCG_STAGE_BYTES
-#define BCG_STAGE_BYTES 8192
+#define BCG_STAGE_BYTES 4096
 #endif
 constexpr int kThreads = BCG_THREADS;    // threads per CTA of the sweep kernel
 constexpr int kWarps = kThreads / 32;    // independent tile workers per CTA
 constexpr int kTileVerts = 32;           // max vertices per tile (one per lane)
-constexpr int kTileEdges = 256;          // max adjacency entries per tile
-constexpr int kItems = kTileEdges / 32;  // edges per lane per tile
+#ifndef BCG_TILE_EDGES
+#define BCG_TILE_EDGES 512
+#endif
+constexpr int kTileEdges = BCG_TILE_EDGES;  // max adjacency entries per tile
+constexpr int kItems = 8;                   // edges per lane in one round of a tile
+constexpr int kRoundEdges = 32 * kItems;    // a warp takes a tile's edges in rounds of this many
+static_assert(kTileEdges % kRoundEdges == 0, "a tile holds whole rounds");
 constexpr int kStageBytes = BCG_STAGE_BYTES;  // per-warp shared staging of gathered rows
 constexpr int kPushSplit = 8;            // sparse push sweeps: warps per tile
 constexpr uint16_t kUnvisited = 0xFFFFu;
@@ -58,8 +63,7 @@ enum : int { kFwdPush = 0, kFwdPull = 1, kBwd = 2 };
 
 // Control block of one kernel launch (zeroed by the host before the launch).
 struct Ctrl {
-    unsigned int bar_count;
-    unsigned int bar_gen;
+    unsigned long long bar_arrived;  // grid barrier arrivals since the launch (monotone)
     int error;      // BCG_ERR_* code set by the device, 0 = fine
     int overflow;   // a uint64 sigma sum wrapped
     unsigned long long wait_ns;  // bound of every device-side wait

@@ -35,10 +35,11 @@ constexpr uint64_t kNaMaxN = BCG_NOALLOC_MAX_VERTICES;
 constexpr uint64_t kNaMaxAdj = BCG_NOALLOC_MAX_ADJ;
 constexpr uint64_t kNaMaxSrc = BCG_NOALLOC_MAX_SOURCES;
 constexpr int kNaMaxWidth = 6;
-// every tile holds at least one non-hub vertex or one 256-entry hub chunk:
-// tiles <= (n - hubs) + sum over hubs of ceil(deg / 256) <= n + adj / 256
+// every tile holds at least one non-hub vertex or one kTileEdges-entry hub
+// chunk: tiles <= (n - hubs) + sum over hubs of ceil(deg / kTileEdges)
+// <= n + adj / kTileEdges
 constexpr uint64_t kNaMaxTiles = kNaMaxN + kNaMaxAdj / kTileEdges;
-constexpr uint64_t kNaMaxHubs = kNaMaxAdj / (kTileEdges + 1) + 1;  // a hub has more than 256 entries
+constexpr uint64_t kNaMaxHubs = kNaMaxAdj / (kTileEdges + 1) + 1;  // a hub has more than kTileEdges entries
 constexpr uint64_t kNaMaxSlots = kNaMaxSrc + kNaMaxWidth;
 constexpr int kNaMaxDevices = 64;
 

@@ -28,12 +28,15 @@
 // while the adjacency streams past with an evict-first policy.
 //
 // Work decomposition.  Vertices are cut into static tiles of <= 32
-// consecutive vertices and <= 256 adjacency entries; a vertex with more than
-// 256 neighbours is split into 256-entry chunks whose partial sums meet in
-// hub_acc (the last chunk to arrive finishes the vertex).  One warp works on
-// one tile at a time with no CTA-wide synchronisation: lane j owns vertex j,
-// the tile's edges are cut into contiguous runs of <= 8 per lane (merge-path
-// over the warp's exclusive scan of active degrees).  Each lane loads its
+// consecutive vertices and <= kTileEdges (512) adjacency entries; a vertex
+// with more entries is split into kTileEdges-entry chunks whose partial sums
+// meet in hub_acc (the last chunk to arrive finishes the vertex).  One warp
+// works on one tile at a time with no CTA-wide synchronisation: lane j owns
+// vertex j, the tile's active edges are taken in rounds of <= 256, and each
+// round is cut into contiguous runs of <= 8 per lane (merge-path over the
+// warp's exclusive scan of active degrees).  A tile's fixed costs (its two
+// list and descriptor reads, row loads, scan and finishing writes) are about
+// two thirds of a dense sweep at 256 entries per tile, hence the larger tiles.  Each lane loads its
 // run's adjacency entries, then issues cp.async copies of all their rows into
 // its slice of the warp's shared staging buffer, so a tile costs two dependent
 // global round trips however many edges are in flight.  Push and backward
@@ -90,25 +93,28 @@ __device__ __forceinline__ void cp_wait_all() {
     asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
 
-// Software grid barrier (all CTAs co-resident: cooperative launch).  Returns
-// false when any CTA recorded an error, in which case the caller returns.
+// Software grid barrier (all CTAs co-resident: cooperative launch).  One
+// atomic per CTA on a monotone arrival counter: the k-th barrier of the
+// launch is complete once the counter reaches k * nblocks, so nothing is
+// reset between barriers.  Thread 0 also reads the error and overflow flags
+// once, after every CTA has arrived, and hands the verdict to its CTA through
+// shared memory.  Returns false when any CTA recorded an error or an overflow,
+// in which case the caller returns.
 __device__ bool grid_sync(Ctrl *c, unsigned int nblocks, unsigned long long wait_ns) {
+    __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned int *genp = &c->bar_gen;
-        unsigned int gen = *genp;
         __threadfence();
-        unsigned int arrived = atomicAdd(&c->bar_count, 1u);
-        if (arrived == nblocks - 1) {
-            atomicExch(&c->bar_count, 0u);
-            __threadfence();
-            atomicAdd(&c->bar_gen, 1u);
-        } else {
+        const unsigned long long arrived = atomicAdd(&c->bar_arrived, 1ull) + 1ull;
+        const unsigned long long target = (arrived + nblocks - 1) / nblocks * nblocks;
+        const volatile unsigned long long *cnt = &c->bar_arrived;
+        const volatile int *err = &c->error;
+        if (arrived != target) {
             unsigned long long t0 = global_ns();
             unsigned int spins = 0;
-            while (*genp == gen) {
+            while (*cnt < target) {
                 if ((++spins & 255u) == 0) {
-                    if (*reinterpret_cast<volatile int *>(&c->error)) break;
+                    if (*err) break;
                     if (global_ns() - t0 > wait_ns) {
                         atomicCAS(&c->error, 0, BCG_ERR_TIMEOUT);
                         break;
@@ -118,9 +124,10 @@ __device__ bool grid_sync(Ctrl *c, unsigned int nblocks, unsigned long long wait
             }
         }
         __threadfence();
+        ok = (*err == 0) && (*reinterpret_cast<volatile int *>(&c->overflow) == 0);
     }
     __syncthreads();
-    return *reinterpret_cast<volatile int *>(&c->error) == 0 && *reinterpret_cast<volatile int *>(&c->overflow) == 0;
+    return ok != 0;
 }
 
 // ---- state-row field access (row words: levels in halfwords, then values)
@@ -166,7 +173,7 @@ struct WarpSmem {
     unsigned long long acc[kTileVerts][S];
     unsigned long long own[kTileVerts][S];
     uint4 stage[kStageBytes / 16];  // rows gathered by cp.async, lane-sliced
-    // the tile's adjacency entries (aligned-down start, <= 256 + 3 entries)
+    // the tile's adjacency entries (aligned-down start, <= kTileEdges + 3 entries)
     alignas(16) uint32_t adjs[kTileEdges + 16];
     // per-warp discovery totals of the sweep (LaneCounts layout)
     unsigned long long cnt[2 + 3 * S];
@@ -433,7 +440,7 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
     // while each lane loads its vertex's row, degree/reach and row start
     const uint32_t ab = T.e0 & ~3u;
     {
-        const uint32_t nch16 = (T.e1 - ab + 3) >> 2;  // <= 65: a tile spans <= 256 entries
+        const uint32_t nch16 = (T.e1 - ab + 3) >> 2;  // <= kTileEdges / 4 + 1
         for (uint32_t c = lane; c < nch16; c += 32) cp_async16_stream(ws.adjs + 4 * c, a.adj + ab + 4 * c, pol);
     }
     uint32_t w[NW];
@@ -485,17 +492,22 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
     if (lane == 0) ws.pre[nv] = total;
     __syncwarp();
 
-    // ---- phase 2: this part's edges, a contiguous run of <= kItems per lane
+    // ---- phase 2: this part's edges [w0, w1), in rounds of <= kRoundEdges;
+    // in each round every lane takes a contiguous run of <= kItems
     uint32_t w0 = 0, w1 = total;
     if (MODE == kFwdPush && x.split > 1) {
         w0 = (uint32_t)(((unsigned long long)total * part) / x.split);
         w1 = (uint32_t)(((unsigned long long)total * (part + 1)) / x.split);
     }
-    if (w1 > w0) {
-        const uint32_t per = (w1 - w0 + 31) / 32;  // <= kItems: a tile holds <= 256 edges
-        const uint32_t i0 = w0 + lane * per;
-        const uint32_t i1 = min(w1, i0 + per);
-        uint32_t j = 0;
+    for (uint32_t r0 = w0; r0 < w1; r0 += kRoundEdges) {
+        const uint32_t r1 = min(w1, r0 + (uint32_t)kRoundEdges);
+        const uint32_t per = (r1 - r0 + 31) / 32;  // <= kItems
+        const uint32_t i0 = r0 + lane * per;
+        const uint32_t i1 = min(r1, i0 + per);
+        // the run's vertex j, the end of its edges (nxt) and the offset of its
+        // edges in adjs (base + i) stay in registers; they are reloaded from
+        // shared memory only when the run crosses into the next vertex
+        uint32_t j = 0, nxt = 0, base = 0;
         if (i0 < i1) {
             uint32_t lo = 0, hi = nv;
             while (hi - lo > 1) {
@@ -503,15 +515,23 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
                 if (ws.pre[mid] <= i0) lo = mid; else hi = mid;
             }
             j = lo;
+            nxt = ws.pre[j + 1];
+            base = ws.eb[j] - ab - ws.pre[j];
         }
         uint32_t jj[kItems], uu[kItems];
 #pragma unroll
         for (int q = 0; q < kItems; ++q) {
             const uint32_t i = i0 + q;
             if (i < i1) {
-                while (i >= ws.pre[j + 1]) ++j;
+                if (i >= nxt) {
+                    do {
+                        ++j;
+                        nxt = ws.pre[j + 1];
+                    } while (i >= nxt);
+                    base = ws.eb[j] - ab - ws.pre[j];
+                }
                 jj[q] = j;
-                uu[q] = ws.adjs[ws.eb[j] - ab + (i - ws.pre[j])];
+                uu[q] = ws.adjs[base + i];
             }
         }
         if (MODE == kFwdPush) {
@@ -573,6 +593,7 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
 #pragma unroll
             for (int k = 0; k < S; ++k) run[k] = 0ull;
             uint32_t runj = (i0 < i1) ? jj[0] : 0u;
+            uint32_t runm = ws.mask[runj];
 #pragma unroll
             for (int r = 0; r < kItems / E; ++r) {
 #pragma unroll
@@ -592,8 +613,9 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
                     if (jj[idx] != runj) {
                         flush_run<S, MODE, EXT>(a, ws, runj, run);
                         runj = jj[idx];
+                        runm = ws.mask[runj];
                     }
-                    const uint32_t jm = ws.mask[jj[idx]];
+                    const uint32_t jm = runm;
                     uint32_t wr[RowGeom<S>::kWords];
 #pragma unroll
                     for (int h = 0; h < H; ++h) {
@@ -903,14 +925,15 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
         // right after a barrier (here: after the init barrier), never at the
         // start of a sweep where a faster CTA may already have appended
         unsigned long long ucur = vload64(&c->uctr);
+        // level d's list: loaded together with the sweep counters right after
+        // each barrier (one round trip per sweep)
+        uint32_t lb = vload32(a.lbase), lc = vload32(a.lcnt);
         for (;;) {
             SweepCtx x;
             x.mode = (!a.directed && (double)pf_cur >= (double)a.push_pull_ratio * (double)pu_cur) ? kFwdPull
                                                                                                     : kFwdPush;
             x.d = d;
             x.D = 0;
-            const uint32_t lb = vload32(a.lbase + d);
-            const uint32_t lc = vload32(a.lcnt + d);
             x.lb_next = lb + lc;
             x.next_lvl = d + 1;
             x.key_next = tile_key(b, d + 1);
@@ -956,9 +979,11 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
             if (!grid_sync(c, nblk, wait_ns)) return;
             const unsigned long long disc = vload64(&c->disc[d & 3]);
             const unsigned long long pfn = vload64(&c->pf[d & 3]);
+            const unsigned long long uafter = vload64(&c->uctr);
+            lb = vload32(a.lbase + d + 1);
+            lc = vload32(a.lcnt + d + 1);
             trace(a, b, x.mode == kFwdPull ? 2u : 1u, d, walked, disc);
             if (x.mode == kFwdPull) {
-                const unsigned long long uafter = vload64(&c->uctr);
                 ustart = ucur;
                 ulen = (uint32_t)(uafter - ucur);
                 ucur = uafter;
@@ -987,6 +1012,9 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
 
         // ---- backward sweeps over the level lists
         const int lowest = a.dbg_delta ? 0 : 1;
+        // the level lists are final: each level's list position is loaded one
+        // sweep ahead
+        uint32_t blb = vload32(a.lbase + D), blc = vload32(a.lcnt + D);
         for (int dd = (int)D; dd >= lowest; --dd) {
             SweepCtx x;
             x.mode = kBwd;
@@ -996,8 +1024,11 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
             x.lb_next = 0;
             x.next_lvl = 0;
             x.split = 1;
-            const uint32_t lb = vload32(a.lbase + dd);
-            const uint32_t lc = vload32(a.lcnt + dd);
+            const uint32_t lb = blb, lc = blc;
+            if (dd > lowest) {
+                blb = vload32(a.lbase + dd - 1);
+                blc = vload32(a.lcnt + dd - 1);
+            }
             if (threadIdx.x == 0) sm.next = 0;
             __syncthreads();
             run_sweep<S, EXT>(a, sm, x, a.lists + lb, 0, lc, 0xFFFFFFFFull);

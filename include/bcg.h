@@ -258,8 +258,8 @@ int bcg_batch_reset_bc(bcg_batch *b);
 int bcg_batch_get_bc(bcg_batch *b, uint32_t graph, double *bc_host);
 
 /* Times the first sample_batches batches (0: 4) of the schedule for each
- * batch width in {1, 3, 6} and each tile shape in {32x256, 32x128, 16x128,
- * 16x64} (vertices x adjacency entries per tile), keeps the fastest per
+ * batch width in {1, 3, 6} and each tile shape in {32x512, 32x256, 32x128,
+ * 16x128, 16x64} (vertices x adjacency entries per tile), keeps the fastest per
  * root and resets the accumulators.  Any output pointer may be NULL. */
 int bcg_batch_autotune(bcg_batch *b, uint32_t sample_batches, uint32_t *width,
                        uint32_t *tile_vertices, uint32_t *tile_entries);

@@ -66,7 +66,7 @@ def test_batch_autotune_keeps_results():
     graphs = _mixed_graphs()[:6]
     with bcg.Batch(graphs) as B:
         w, tv, te = B.autotune(sample_batches=2)
-        assert w in (1, 3, 6) and (tv, te) in ((32, 256), (32, 128), (16, 128), (16, 64))
+        assert w in (1, 3, 6) and (tv, te) in ((32, 512), (32, 256), (32, 128), (16, 128), (16, 64))
         assert not B.bc(0).any()  # tuning runs are not left in the accumulators
         info = B.info()
         assert (info["width"], info["tile_vertices"], info["tile_entries"]) == (w, tv, te)
