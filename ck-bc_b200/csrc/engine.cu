@@ -126,14 +126,15 @@ __global__ void k_levels_out(uint32_t n, const unsigned char *__restrict__ rows,
 // entries; a vertex with more than ecap entries is split into ecap-entry
 // chunks (vcap <= 32, ecap <= kTileEdges: the sweep kernel's lane and
 // staging limits).
-// A tile never spans a vertex listed in `breaks` (sorted) and the vertex
-// before it.  tile_of[v] = index of v's tile (of its first chunk, with
+// Only vertices [0, tn) get tiles.  A tile never spans a vertex listed in
+// `breaks` (sorted) and the vertex before it.  tile_of[v] = index of v's tile (of its first chunk, with
 // kHubFlag, when v is split).
-static void build_tiles(const uint32_t *offs, uint32_t n, uint32_t vcap, uint32_t ecap,
+static void build_tiles(const uint32_t *offs, uint32_t n, uint32_t tn, uint32_t vcap, uint32_t ecap,
                         const std::vector<uint32_t> &breaks, std::vector<Tile> &tiles, uint32_t &nhub,
                         std::vector<uint32_t> &tile_of) {
     tiles.clear();
-    tile_of.assign(n, 0);
+    tile_of.assign(n, 0);  // vertices past tn (no edges: never reached) keep tile 0
+    n = tn;
     nhub = 0;
     uint32_t v = 0;
     size_t nb = 0;  // next break point
@@ -193,6 +194,7 @@ static void graph_free(bcg_graph *g) {
     cudaFree(g->d_tile_of); cudaFree(g->d_tmark); cudaFree(g->d_lists);
     cudaFree(g->d_lbase); cudaFree(g->d_lcnt); cudaFree(g->d_ulist); cudaFree(g->d_bc_save);
     cudaFree(g->d_tree_acc);
+    cudaFree(g->d_ext);
     cudaFree(g->d_rows); cudaFree(g->d_ctrl);
     cudaFree(g->d_roots); cudaFree(g->d_pend); cudaFree(g->d_mult); cudaFree(g->d_rstat);
     if (g->ev0) cudaEventDestroy(g->ev0);
@@ -256,7 +258,8 @@ static int setup_tiles(bcg_graph *g, const uint32_t *h_offs) {
     const uint32_t n = g->n;
     std::vector<Tile> tiles;
     std::vector<uint32_t> tile_of;
-    build_tiles(h_offs, n, g->tile_vcap, g->tile_ecap, g->tile_breaks, tiles, g->nhub, tile_of);
+    build_tiles(h_offs, n, g->tile_n ? g->tile_n : n, g->tile_vcap, g->tile_ecap, g->tile_breaks, tiles, g->nhub,
+                tile_of);
     g->ntiles = (uint32_t)tiles.size();
     CK(cudaMalloc(&g->d_tiles, std::max<size_t>(1, tiles.size()) * sizeof(Tile)));
     if (!tiles.empty())
@@ -399,7 +402,7 @@ static int plan_run(const bcg_graph *g, const uint32_t *src, uint64_t nsrc, RunP
         if (it == idx.end()) {
             k = (uint32_t)p.roots.size();
             idx.emplace(r, k);
-            p.roots.push_back(r);
+            p.roots.push_back(g->h_intl.empty() ? r : g->h_intl[r]);
             p.pend.push_back(0);
             p.mult.push_back(0.0);
             p.count.push_back(0);
@@ -411,6 +414,32 @@ static int plan_run(const bcg_graph *g, const uint32_t *src, uint64_t nsrc, RunP
         if (r != s && !g->trees) p.pend[k] += 1;
     }
     return BCG_OK;
+}
+
+// BatchArgs fields common to every launch on g.
+static void fill_args(bcg_graph *g, BatchArgs &a) {
+    a.n = g->tile_n ? g->tile_n : g->n;
+    a.ext = g->d_ext;
+    a.offs = g->d_offs;
+    a.adj = g->d_adj;
+    a.vinfo = g->d_vinfo;
+    a.tiles = g->d_tiles;
+    a.ntiles = g->ntiles;
+    a.tile_of = g->d_tile_of;
+    a.tmark = g->d_tmark;
+    a.lists = g->d_lists;
+    a.list_cap = g->list_cap;
+    a.ulist = g->d_ulist;
+    a.lbase = g->d_lbase;
+    a.lcnt = g->d_lcnt;
+    a.rows = g->d_rows;
+    a.bc = g->d_bc;
+    a.hub_acc = g->d_hub_acc;
+    a.hub_cnt = g->d_hub_cnt;
+    a.ctrl = g->d_ctrl;
+    a.nnz = g->nnz_pruned;
+    a.push_pull_ratio = g->ratio;
+    a.directed = (g->flags & BCG_DIRECTED) ? 1 : 0;
 }
 
 static int run_plan(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *stats, bool debug,
@@ -437,27 +466,7 @@ static int run_plan(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *
     CK(cudaMemsetAsync(g->d_hub_acc, 0, (size_t)std::max(1u, g->nhub) * g->state_width * sizeof(unsigned long long), st));
     CK(cudaMemsetAsync(g->d_hub_cnt, 0, (size_t)std::max(1u, g->nhub) * sizeof(unsigned int), st));
     BatchArgs a{};
-    a.n = g->n;
-    a.offs = g->d_offs;
-    a.adj = g->d_adj;
-    a.vinfo = g->d_vinfo;
-    a.tiles = g->d_tiles;
-    a.ntiles = g->ntiles;
-    a.tile_of = g->d_tile_of;
-    a.tmark = g->d_tmark;
-    a.lists = g->d_lists;
-    a.list_cap = g->list_cap;
-    a.ulist = g->d_ulist;
-    a.lbase = g->d_lbase;
-    a.lcnt = g->d_lcnt;
-    a.rows = g->d_rows;
-    a.bc = g->d_bc;
-    a.hub_acc = g->d_hub_acc;
-    a.hub_cnt = g->d_hub_cnt;
-    a.ctrl = g->d_ctrl;
-    a.nnz = g->nnz_pruned;
-    a.push_pull_ratio = g->ratio;
-    a.directed = (g->flags & BCG_DIRECTED) ? 1 : 0;
+    fill_args(g, a);
     a.dbg_sigma = dbg_sigma;
     a.dbg_delta = dbg_delta;
     // optional per-sweep trace: BCG_TRACE_FILE=<path> appends one CSV line per
@@ -576,31 +585,6 @@ static int run_plan(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *
     return BCG_OK;
 }
 
-// BatchArgs fields common to every launch on g.
-static void fill_args(bcg_graph *g, BatchArgs &a) {
-    a.n = g->n;
-    a.offs = g->d_offs;
-    a.adj = g->d_adj;
-    a.vinfo = g->d_vinfo;
-    a.tiles = g->d_tiles;
-    a.ntiles = g->ntiles;
-    a.tile_of = g->d_tile_of;
-    a.tmark = g->d_tmark;
-    a.lists = g->d_lists;
-    a.list_cap = g->list_cap;
-    a.ulist = g->d_ulist;
-    a.lbase = g->d_lbase;
-    a.lcnt = g->d_lcnt;
-    a.rows = g->d_rows;
-    a.bc = g->d_bc;
-    a.hub_acc = g->d_hub_acc;
-    a.hub_cnt = g->d_hub_cnt;
-    a.ctrl = g->d_ctrl;
-    a.nnz = g->nnz_pruned;
-    a.push_pull_ratio = g->ratio;
-    a.directed = (g->flags & BCG_DIRECTED) ? 1 : 0;
-}
-
 int enqueue_packed(bcg_graph *g, const PackedRun &p, uint32_t S, cudaStream_t st) {
     if (p.nbatch == 0) return BCG_OK;
     // tile marks key on the batch index modulo 2^16 (one launch, <= 65535 batches)
@@ -678,7 +662,8 @@ static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint3
     // iterated pendant-tree pruning: the device holds the kept graph only
     const bool trees = (flags & BCG_PRUNE_TREES) && !(flags & BCG_DIRECTED);
     bcg::TreeInfo tinfo;
-    std::vector<uint32_t> core_offs, core_adj, h_adj_copy;
+    std::vector<uint32_t> core_offs, core_adj, h_adj_copy, ext, intl, lab_offs, lab_adj;
+    uint32_t nlive = 0;
     const uint32_t *orig_offs = ho;
     if (trees) {
         const uint32_t *hadj = adj;
@@ -691,9 +676,10 @@ static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint3
             hadj = h_adj_copy.data();
         }
         peel_trees(ho, hadj, n, tinfo, core_offs, core_adj);
-        offsets = core_offs.data();
-        adj = core_adj.data();
-        ho = core_offs.data();
+        nlive = relabel_live(core_offs, core_adj, n, ext, intl, lab_offs, lab_adj);
+        offsets = lab_offs.data();
+        adj = lab_adj.data();
+        ho = lab_offs.data();
         device_in = false;
         flags &= ~BCG_PRUNE_DEGREE1;
     }
@@ -712,6 +698,7 @@ static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint3
             g->tile_ecap = te;
         }
     }
+    if (trees) g->tile_n = nlive ? nlive : 1;
     auto fail = [&](int code) { graph_free(g); return code; };
     cudaError_t e;
     if ((e = cudaMalloc(&g->d_offs, ((size_t)n + 1) * sizeof(uint32_t))) != cudaSuccess ||
@@ -731,17 +718,25 @@ static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint3
         // skip test, and every kept vertex weighted by its trees (reach)
         g->trees = true;
         g->nnz = nnz;
-        g->h_cdeg = g->h_deg;
-        for (uint32_t v = 0; v < n; ++v) g->h_deg[v] = orig_offs[v + 1] - orig_offs[v];
+        g->h_cdeg.resize(n);
+        for (uint32_t v = 0; v < n; ++v) {
+            g->h_cdeg[v] = core_offs[v + 1] - core_offs[v];
+            g->h_deg[v] = orig_offs[v + 1] - orig_offs[v];
+        }
         g->tinfo = std::move(tinfo);
         g->h_anchor = g->tinfo.anchor;
         g->npruned = (uint32_t)g->tinfo.order.size();
-        std::vector<uint2> vi(n);
-        for (uint32_t v = 0; v < n; ++v)
-            vi[v] = make_uint2(g->h_cdeg[v], g->tinfo.parent[v] == kNoRoot ? g->tinfo.sz[v] - 1 : 0u);
+        std::vector<uint2> vi(n);  // internal numbering
+        for (uint32_t i = 0; i < n; ++i) {
+            const uint32_t v = ext[i];
+            vi[i] = make_uint2(g->h_cdeg[v], g->tinfo.parent[v] == kNoRoot ? g->tinfo.sz[v] - 1 : 0u);
+        }
         if ((e = cudaMemcpy(g->d_vinfo, vi.data(), (size_t)n * sizeof(uint2), cudaMemcpyHostToDevice)) != cudaSuccess ||
-            (e = cudaMalloc(&g->d_tree_acc, (size_t)n * sizeof(double))) != cudaSuccess)
+            (e = cudaMalloc(&g->d_tree_acc, (size_t)n * sizeof(double))) != cudaSuccess ||
+            (e = cudaMalloc(&g->d_ext, (size_t)n * sizeof(uint32_t))) != cudaSuccess ||
+            (e = cudaMemcpy(g->d_ext, ext.data(), (size_t)n * sizeof(uint32_t), cudaMemcpyHostToDevice)) != cudaSuccess)
             return fail(set_error(BCG_ERR_CUDA, "tree weights: %s", cudaGetErrorString(e)));
+        g->h_intl = std::move(intl);
     }
     *out = g;
     return BCG_OK;

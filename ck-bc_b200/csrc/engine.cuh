@@ -98,7 +98,7 @@ struct RootStat {
 };
 
 struct BatchArgs {
-    uint32_t n;
+    uint32_t n;             // vertices with state rows a sweep may touch (the tiles' range)
     const uint32_t *offs;   // CSR row starts (n+1); pruned lists start here too
     const uint32_t *adj;    // adjacency (pruned lists compacted to the front)
     const uint2 *vinfo;     // per vertex {deg in the pruned graph, reach}
@@ -113,6 +113,7 @@ struct BatchArgs {
     uint32_t *ulist;        // ring of 2 * ntiles: tiles that still hold unvisited vertices
     unsigned char *rows;    // n state rows of row_bytes(S)
     double *bc;             // n accumulators
+    const uint32_t *ext;    // vertex v's bc is bc[ext[v]] (nullptr: bc[v])
     const uint32_t *roots;  // nbatch * S, kNoRoot = empty slot
     const double *mult;     // nbatch * S weight of each root's dependencies
     const uint32_t *pend;   // nbatch * S pendant sources folded into the root

@@ -60,7 +60,14 @@ struct bcg_graph {
     float ratio = 0.2f;
     bool trees = false;               // BCG_PRUNE_TREES: pendant trees folded (tinfo)
     bcg::TreeInfo tinfo;
-    std::vector<uint32_t> h_cdeg;     // degrees in the kept graph (trees mode)
+    std::vector<uint32_t> h_cdeg;     // degrees in the kept graph, caller's numbering (trees mode)
+    // Trees mode numbers the searched vertices internally: the vertices with
+    // kept edges first (caller's order), then the rest, so the tiles cover
+    // [0, tile_n) only.  h_intl: caller's id -> internal id; d_ext: internal
+    // id -> caller's id, where the sweep adds each vertex's bc.
+    uint32_t tile_n = 0;              // vertices covered by tiles (0: all n)
+    std::vector<uint32_t> h_intl;     // empty: internal ids are the caller's
+    uint32_t *d_ext = nullptr;
     double *d_tree_acc = nullptr;     // tree vertices' closed-form bc of one run
     int sigma_mode = 0;               // 0 auto (exact, extended on overflow), 1 exact only, 2 extended
     double *d_bc_save = nullptr;      // accumulators before an automatic-mode run
@@ -96,6 +103,12 @@ int graph_retile(bcg_graph *g, uint32_t vcap, uint32_t ecap, bool force = false)
 // Peels every pendant tree off the graph (t) and returns the kept graph's CSR.
 void peel_trees(const uint32_t *offs, const uint32_t *adj, uint32_t n, TreeInfo &t,
                 std::vector<uint32_t> &core_offs, std::vector<uint32_t> &core_adj);
+// Renumbers a graph so the vertices with edges come first (in their order),
+// then the rest: ext[i] = old id of new vertex i, intl = its inverse; the
+// renumbered CSR is (offs2, adj2).  Returns the number of vertices with edges.
+uint32_t relabel_live(const std::vector<uint32_t> &offs, const std::vector<uint32_t> &adj, uint32_t n,
+                      std::vector<uint32_t> &ext, std::vector<uint32_t> &intl, std::vector<uint32_t> &offs2,
+                      std::vector<uint32_t> &adj2);
 // Closed-form bc of the tree vertices (and the anchors' tree terms) for the
 // source multiplicities cnt[v].
 void tree_bc(const TreeInfo &t, const std::vector<uint32_t> &cnt, std::vector<double> &acc);

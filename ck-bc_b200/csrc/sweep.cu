@@ -697,7 +697,7 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
                 if (d > 0) add += sm.mult[k] * delta;
                 if (a.dbg_delta) a.dbg_delta[v] = delta;
             }
-            if (d > 0) a.bc[v] += add;
+            if (d > 0) a.bc[a.ext ? a.ext[v] : v] += add;
         }
     }
     if (MODE == kFwdPull) {
@@ -1044,7 +1044,7 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
                 const size_t idx = (size_t)b * S + k;
                 const unsigned long long W = vload64(&c->wsum[k]);
                 const uint32_t p = packed ? 0u : a.pend[idx];
-                if (p && W >= 2) a.bc[r] += (double)p * (double)(W - 2);
+                if (p && W >= 2) a.bc[a.ext ? a.ext[r] : r] += (double)p * (double)(W - 2);
                 a.rstat[idx].visited = vload64(&c->visited[k]);
                 a.rstat[idx].wsum = W;
                 a.rstat[idx].mc2 = vload64(&c->mc2[k]);

@@ -101,6 +101,31 @@ void peel_trees(const uint32_t *offs, const uint32_t *adj, uint32_t n, TreeInfo 
     }
 }
 
+uint32_t relabel_live(const std::vector<uint32_t> &offs, const std::vector<uint32_t> &adj, uint32_t n,
+                      std::vector<uint32_t> &ext, std::vector<uint32_t> &intl, std::vector<uint32_t> &offs2,
+                      std::vector<uint32_t> &adj2) {
+    ext.resize(n);
+    intl.resize(n);
+    uint32_t nlive = 0;
+    for (uint32_t v = 0; v < n; ++v)
+        if (offs[v + 1] > offs[v]) ext[nlive++] = v;
+    uint32_t k = nlive;
+    for (uint32_t v = 0; v < n; ++v)
+        if (offs[v + 1] == offs[v]) ext[k++] = v;
+    for (uint32_t i = 0; i < n; ++i) intl[ext[i]] = i;
+    offs2.assign((size_t)n + 1, 0);
+    for (uint32_t i = 0; i < n; ++i) offs2[i + 1] = offs2[i] + (offs[ext[i] + 1] - offs[ext[i]]);
+    adj2.resize(adj.size());
+    // ids keep their relative order, so sorted lists stay sorted
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (int64_t i = 0; i < (int64_t)nlive; ++i) {
+        const uint32_t v = ext[i];
+        uint32_t *dst = adj2.data() + offs2[i];
+        for (uint32_t e = offs[v]; e < offs[v + 1]; ++e) *dst++ = intl[adj[e]];
+    }
+    return nlive;
+}
+
 void tree_bc(const TreeInfo &t, const std::vector<uint32_t> &cnt, std::vector<double> &acc) {
     const size_t n = t.parent.size();
     // sources per component and per subtree (a vertex's own count included)

@@ -88,3 +88,55 @@ def test_peeling_anchors_and_core(harness):
     assert core_nnz == 6 and peeled == 5  # 3, 4, 5, 6 and one end of the isolated edge
     assert anchor.tolist()[:7] == [0, 1, 2, 2, 2, 1, 1]
     assert anchor[7] == anchor[8] and anchor[7] in (7, 8)
+
+
+RELABEL = r"""
+#include <cstdio>
+#include <vector>
+#include "engine_internal.hpp"
+using namespace bcg;
+int main() {
+    unsigned n, m;
+    if (scanf("%u %u", &n, &m) != 2) return 1;
+    std::vector<uint32_t> offs(n + 1), adj(m);
+    for (auto &x : offs) scanf("%u", &x);
+    for (auto &x : adj) scanf("%u", &x);
+    TreeInfo t;
+    std::vector<uint32_t> co, ca, ext, intl, o2, a2;
+    peel_trees(offs.data(), adj.data(), n, t, co, ca);
+    const uint32_t nlive = relabel_live(co, ca, n, ext, intl, o2, a2);
+    printf("%u\n", nlive);
+    for (auto x : co) printf("%u ", x); printf("\n");
+    for (auto x : ca) printf("%u ", x); printf("\n");
+    for (auto x : ext) printf("%u ", x); printf("\n");
+    for (auto x : o2) printf("%u ", x); printf("\n");
+    for (auto x : a2) printf("%u ", x); printf("\n");
+}
+"""
+
+
+def test_relabel_keeps_the_kept_graph(tmp_path):
+    """The searched graph is renumbered with its vertices that have edges
+    first, in their original order; the renumbered CSR is the same graph."""
+    (tmp_path / "r.cpp").write_text(RELABEL)
+    exe = tmp_path / "r"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "ck-bc_b200", "csrc"), "-I",
+                    os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include",
+                    os.path.join(ROOT, "ck-bc_b200", "csrc", "trees.cpp"), str(tmp_path / "r.cpp"), "-o", str(exe)],
+                   check=True)
+    offs, adj = bcg.generate("rmat:scale=9,ef=4,seed=5,pendant_frac=0.3,pendant_mean=5")
+    n = len(offs) - 1
+    txt = f"{n} {len(adj)}\n" + " ".join(map(str, offs)) + "\n" + " ".join(map(str, adj)) + "\n"
+    out = subprocess.run([str(exe)], input=txt, capture_output=True, text=True, check=True).stdout.split("\n")
+    nlive = int(out[0])
+    co, ca, ext, o2, a2 = (np.array(out[i].split(), dtype=np.int64) for i in range(1, 6))
+    cdeg = np.diff(co)
+    assert nlive == int((cdeg > 0).sum()) and 0 < nlive < n
+    assert sorted(ext.tolist()) == list(range(n))
+    assert np.all(cdeg[ext[:nlive]] > 0) and np.all(cdeg[ext[nlive:]] == 0)
+    assert np.all(np.diff(ext[:nlive]) > 0)  # original order kept
+    intl = np.empty(n, dtype=np.int64)
+    intl[ext] = np.arange(n)
+    for i in range(n):
+        v = ext[i]
+        assert a2[o2[i]:o2[i + 1]].tolist() == intl[ca[co[v]:co[v + 1]]].tolist()
