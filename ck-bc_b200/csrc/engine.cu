@@ -187,6 +187,7 @@ static void graph_free(bcg_graph *g) {
     if (!g) return;
     int cur = -1;
     cudaGetDevice(&cur);
+    if (g->comp_job.valid()) g->comp_job.wait();
     if (cur != g->device) cudaSetDevice(g->device);
     cudaFree(g->d_offs); cudaFree(g->d_adj); cudaFree(g->d_vinfo);
     cudaFree(g->d_anchor); cudaFree(g->d_reach); cudaFree(g->d_bc);
@@ -341,10 +342,17 @@ static int check_device() {
 
 static int validate_csr(const uint32_t *offs, const uint32_t *adj, uint32_t n, uint64_t nnz) {
     if (offs[0] != 0 || offs[n] != nnz) return set_error(BCG_ERR_ARG, "offsets[0] must be 0 and offsets[n] == nnz");
-    for (uint32_t v = 0; v < n; ++v)
-        if (offs[v + 1] < offs[v]) return set_error(BCG_ERR_ARG, "offsets not non-decreasing at %u", v);
-    for (uint64_t e = 0; e < nnz; ++e)
-        if (adj[e] >= n) return set_error(BCG_ERR_ARG, "adj[%" PRIu64 "] = %u >= n", e, adj[e]);
+    uint64_t bad_offs = 0, bad_adj = 0;
+#pragma omp parallel for reduction(+ : bad_offs) schedule(static)
+    for (int64_t v = 0; v < (int64_t)n; ++v) bad_offs += offs[v + 1] < offs[v];
+#pragma omp parallel for reduction(+ : bad_adj) schedule(static)
+    for (int64_t e = 0; e < (int64_t)nnz; ++e) bad_adj += adj[e] >= n;
+    if (bad_offs)
+        for (uint32_t v = 0; v < n; ++v)
+            if (offs[v + 1] < offs[v]) return set_error(BCG_ERR_ARG, "offsets not non-decreasing at %u", v);
+    if (bad_adj)
+        for (uint64_t e = 0; e < nnz; ++e)
+            if (adj[e] >= n) return set_error(BCG_ERR_ARG, "adj[%" PRIu64 "] = %u >= n", e, adj[e]);
     return BCG_OK;
 }
 
@@ -366,6 +374,8 @@ __global__ void k_add(uint32_t n, double *__restrict__ bc, const double *__restr
 // terms) for this run's sources, added on the device after the search.
 static int add_tree_terms(bcg_graph *g, const uint32_t *src, uint64_t nsrc, const RunPlan &p, cudaStream_t st,
                           bcg_stats *stats) {
+    if (g->comp_job.valid() && g->comp_job.get() != BCG_OK)
+        return set_error(BCG_ERR_OOM, "labelling the components: out of host memory");
     std::vector<uint32_t> cnt(g->n, 0);
     for (uint64_t i = 0; i < nsrc; ++i)
         if (g->h_deg[src[i]]) ++cnt[src[i]];
@@ -392,9 +402,10 @@ static int plan_run(const bcg_graph *g, const uint32_t *src, uint64_t nsrc, RunP
         const uint32_t r = g->h_anchor.empty() ? s : g->h_anchor[s];
         if (g->trees && g->h_cdeg[r] == 0) {
             // a tree component: no kept edges, its bc is all in the tree terms
+            // (the kept vertex r is the last one of its tree: sz[r] is the component)
             ++p.tree_only;
-            p.tree_edges += g->tinfo.comp_n[g->tinfo.comp[s]] - 1;
-            p.tree_verts += g->tinfo.comp_n[g->tinfo.comp[s]];
+            p.tree_edges += g->tinfo.sz[r] - 1;
+            p.tree_verts += g->tinfo.sz[r];
             continue;
         }
         auto it = idx.find(r);
@@ -662,7 +673,7 @@ static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint3
     // iterated pendant-tree pruning: the device holds the kept graph only
     const bool trees = (flags & BCG_PRUNE_TREES) && !(flags & BCG_DIRECTED);
     bcg::TreeInfo tinfo;
-    std::vector<uint32_t> core_offs, core_adj, h_adj_copy, ext, intl, lab_offs, lab_adj;
+    std::vector<uint32_t> cdeg, h_adj_copy, ext, intl, lab_offs, lab_adj;
     uint32_t nlive = 0;
     const uint32_t *orig_offs = ho;
     if (trees) {
@@ -675,15 +686,14 @@ static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint3
                 if (h_adj_copy[e] >= n) return set_error(BCG_ERR_ARG, "adj[%" PRIu64 "] = %u >= n", e, h_adj_copy[e]);
             hadj = h_adj_copy.data();
         }
-        peel_trees(ho, hadj, n, tinfo, core_offs, core_adj);
-        nlive = relabel_live(core_offs, core_adj, n, ext, intl, lab_offs, lab_adj);
+        nlive = peel_trees(ho, hadj, n, tinfo, cdeg, ext, intl, lab_offs, lab_adj);
         offsets = lab_offs.data();
         adj = lab_adj.data();
         ho = lab_offs.data();
         device_in = false;
         flags &= ~BCG_PRUNE_DEGREE1;
     }
-    const uint64_t dev_nnz = trees ? core_adj.size() : nnz;
+    const uint64_t dev_nnz = trees ? lab_adj.size() : nnz;
     bcg_graph *g = new bcg_graph();
     cudaGetDevice(&g->device);
     g->n = n;
@@ -718,11 +728,8 @@ static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint3
         // skip test, and every kept vertex weighted by its trees (reach)
         g->trees = true;
         g->nnz = nnz;
-        g->h_cdeg.resize(n);
-        for (uint32_t v = 0; v < n; ++v) {
-            g->h_cdeg[v] = core_offs[v + 1] - core_offs[v];
-            g->h_deg[v] = orig_offs[v + 1] - orig_offs[v];
-        }
+        g->h_cdeg = std::move(cdeg);
+        for (uint32_t v = 0; v < n; ++v) g->h_deg[v] = orig_offs[v + 1] - orig_offs[v];
         g->tinfo = std::move(tinfo);
         g->h_anchor = g->tinfo.anchor;
         g->npruned = (uint32_t)g->tinfo.order.size();
@@ -737,6 +744,18 @@ static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint3
             (e = cudaMemcpy(g->d_ext, ext.data(), (size_t)n * sizeof(uint32_t), cudaMemcpyHostToDevice)) != cudaSuccess)
             return fail(set_error(BCG_ERR_CUDA, "tree weights: %s", cudaGetErrorString(e)));
         g->h_intl = std::move(intl);
+        g->h_lab_offs = std::move(lab_offs);
+        g->h_lab_adj = std::move(lab_adj);
+        g->comp_job = std::async(std::launch::async, [g]() {
+            try {
+                label_components(g->h_lab_offs.data(), g->h_lab_adj.data(), g->n, g->h_intl, g->tinfo);
+            } catch (...) {
+                return (int)BCG_ERR_OOM;
+            }
+            std::vector<uint32_t>().swap(g->h_lab_offs);
+            std::vector<uint32_t>().swap(g->h_lab_adj);
+            return (int)BCG_OK;
+        });
     }
     *out = g;
     return BCG_OK;

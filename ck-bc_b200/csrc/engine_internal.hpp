@@ -2,6 +2,7 @@
 // translation units (engine.cu: single graphs; batch.cu: packed unions of
 // graphs).  Not part of the public ABI.
 #pragma once
+#include <future>
 #include <vector>
 
 #include "bcg.h"
@@ -68,6 +69,11 @@ struct bcg_graph {
     uint32_t tile_n = 0;              // vertices covered by tiles (0: all n)
     std::vector<uint32_t> h_intl;     // empty: internal ids are the caller's
     uint32_t *d_ext = nullptr;
+    // trees mode: the components are labelled on a host thread that overlaps
+    // the first run's searches (from a copy of the kept graph's CSR); the
+    // closed-form tree terms wait for it
+    std::vector<uint32_t> h_lab_offs, h_lab_adj;
+    std::future<int> comp_job;
     double *d_tree_acc = nullptr;     // tree vertices' closed-form bc of one run
     int sigma_mode = 0;               // 0 auto (exact, extended on overflow), 1 exact only, 2 extended
     double *d_bc_save = nullptr;      // accumulators before an automatic-mode run
@@ -100,15 +106,19 @@ int enqueue_packed(bcg_graph *g, const PackedRun &p, uint32_t S, cudaStream_t st
 int check_ctrl(bcg_graph *g, cudaStream_t st);
 // Rebuilds the work tiles with another shape (vcap vertices, ecap entries).
 int graph_retile(bcg_graph *g, uint32_t vcap, uint32_t ecap, bool force = false);
-// Peels every pendant tree off the graph (t) and returns the kept graph's CSR.
-void peel_trees(const uint32_t *offs, const uint32_t *adj, uint32_t n, TreeInfo &t,
-                std::vector<uint32_t> &core_offs, std::vector<uint32_t> &core_adj);
-// Renumbers a graph so the vertices with edges come first (in their order),
-// then the rest: ext[i] = old id of new vertex i, intl = its inverse; the
-// renumbered CSR is (offs2, adj2).  Returns the number of vertices with edges.
-uint32_t relabel_live(const std::vector<uint32_t> &offs, const std::vector<uint32_t> &adj, uint32_t n,
-                      std::vector<uint32_t> &ext, std::vector<uint32_t> &intl, std::vector<uint32_t> &offs2,
-                      std::vector<uint32_t> &adj2);
+// Peels every pendant tree off the graph (t: all but the components) and
+// returns the kept graph renumbered so the vertices that keep an edge come
+// first (in their order), then the rest: ext[i] = id of internal vertex i,
+// intl its inverse, (offs2, adj2) the renumbered CSR, cdeg[v] = v's degree
+// in the kept graph.  Returns the number of vertices that keep an edge.
+uint32_t peel_trees(const uint32_t *offs, const uint32_t *adj, uint32_t n, TreeInfo &t, std::vector<uint32_t> &cdeg,
+                    std::vector<uint32_t> &ext, std::vector<uint32_t> &intl, std::vector<uint32_t> &offs2,
+                    std::vector<uint32_t> &adj2);
+// Labels the components of every vertex (t.comp, t.comp_n) from the kept
+// graph's CSR (internal ids; intl: id -> internal id, empty: the same) and
+// the anchors.
+void label_components(const uint32_t *offs, const uint32_t *adj, uint32_t n, const std::vector<uint32_t> &intl,
+                      TreeInfo &t);
 // Closed-form bc of the tree vertices (and the anchors' tree terms) for the
 // source multiplicities cnt[v].
 void tree_bc(const TreeInfo &t, const std::vector<uint32_t> &cnt, std::vector<double> &acc);

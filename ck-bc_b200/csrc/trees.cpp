@@ -8,6 +8,9 @@
 // trees rooted at the remaining ("core") vertices, their anchors.  A component
 // that is a tree keeps one vertex, the last one peeled to degree 0.
 //
+// Components: a tree vertex's component is its anchor's, so the components
+// are labelled on the kept graph alone (label_components).
+//
 // Exactness (ordered pairs (s, t), s a requested source):
 //   - A path between two vertices of one tree, or between a tree vertex and
 //     anything outside its tree, is unique inside the tree and enters the
@@ -32,8 +35,9 @@
 
 namespace bcg {
 
-void peel_trees(const uint32_t *offs, const uint32_t *adj, uint32_t n, TreeInfo &t,
-                std::vector<uint32_t> &core_offs, std::vector<uint32_t> &core_adj) {
+uint32_t peel_trees(const uint32_t *offs, const uint32_t *adj, uint32_t n, TreeInfo &t, std::vector<uint32_t> &cdeg,
+                    std::vector<uint32_t> &ext, std::vector<uint32_t> &intl, std::vector<uint32_t> &offs2,
+                    std::vector<uint32_t> &adj2) {
     std::vector<uint32_t> deg(n);
     for (uint32_t v = 0; v < n; ++v) deg[v] = offs[v + 1] - offs[v];
     t.parent.assign(n, kNoRoot);
@@ -68,62 +72,91 @@ void peel_trees(const uint32_t *offs, const uint32_t *adj, uint32_t n, TreeInfo 
         const uint32_t p = t.parent[v];
         t.anchor[v] = removed[p] ? t.anchor[p] : p;
     }
-    // connected components of the input graph
-    t.comp.assign(n, kNoRoot);
-    t.comp_n.clear();
-    std::vector<uint32_t> stack;
-    for (uint32_t s = 0; s < n; ++s) {
-        if (t.comp[s] != kNoRoot) continue;
-        const uint32_t c = (uint32_t)t.comp_n.size();
-        uint64_t cnt = 0;
-        t.comp[s] = c;
-        stack.push_back(s);
-        while (!stack.empty()) {
-            const uint32_t v = stack.back();
-            stack.pop_back();
-            ++cnt;
-            for (uint32_t e = offs[v]; e < offs[v + 1]; ++e)
-                if (t.comp[adj[e]] == kNoRoot) {
-                    t.comp[adj[e]] = c;
-                    stack.push_back(adj[e]);
-                }
-        }
-        t.comp_n.push_back(cnt);
-    }
-    // the core: every edge between two kept vertices
-    core_offs.assign((size_t)n + 1, 0);
-    core_adj.clear();
-    for (uint32_t v = 0; v < n; ++v) {
+    // the kept graph, renumbered: the kept vertices that keep an edge come
+    // first (in their order), then the rest; ids keep their relative order,
+    // so sorted lists stay sorted (count, number, scan, fill)
+    cdeg.assign(n, 0);
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (int64_t vi = 0; vi < (int64_t)n; ++vi) {
+        const uint32_t v = (uint32_t)vi;
+        uint32_t c = 0;
         if (!removed[v])
-            for (uint32_t e = offs[v]; e < offs[v + 1]; ++e)
-                if (!removed[adj[e]]) core_adj.push_back(adj[e]);
-        core_offs[v + 1] = (uint32_t)core_adj.size();
+            for (uint32_t e = offs[v]; e < offs[v + 1]; ++e) c += !removed[adj[e]];
+        cdeg[v] = c;
     }
-}
-
-uint32_t relabel_live(const std::vector<uint32_t> &offs, const std::vector<uint32_t> &adj, uint32_t n,
-                      std::vector<uint32_t> &ext, std::vector<uint32_t> &intl, std::vector<uint32_t> &offs2,
-                      std::vector<uint32_t> &adj2) {
     ext.resize(n);
     intl.resize(n);
     uint32_t nlive = 0;
     for (uint32_t v = 0; v < n; ++v)
-        if (offs[v + 1] > offs[v]) ext[nlive++] = v;
+        if (cdeg[v]) ext[nlive++] = v;
     uint32_t k = nlive;
     for (uint32_t v = 0; v < n; ++v)
-        if (offs[v + 1] == offs[v]) ext[k++] = v;
+        if (!cdeg[v]) ext[k++] = v;
     for (uint32_t i = 0; i < n; ++i) intl[ext[i]] = i;
     offs2.assign((size_t)n + 1, 0);
-    for (uint32_t i = 0; i < n; ++i) offs2[i + 1] = offs2[i] + (offs[ext[i] + 1] - offs[ext[i]]);
-    adj2.resize(adj.size());
-    // ids keep their relative order, so sorted lists stay sorted
+    for (uint32_t i = 0; i < n; ++i) offs2[i + 1] = offs2[i] + cdeg[ext[i]];
+    adj2.resize(offs2[n]);
 #pragma omp parallel for schedule(dynamic, 4096)
     for (int64_t i = 0; i < (int64_t)nlive; ++i) {
         const uint32_t v = ext[i];
         uint32_t *dst = adj2.data() + offs2[i];
-        for (uint32_t e = offs[v]; e < offs[v + 1]; ++e) *dst++ = intl[adj[e]];
+        for (uint32_t e = offs[v]; e < offs[v + 1]; ++e)
+            if (!removed[adj[e]]) *dst++ = intl[adj[e]];
     }
     return nlive;
+}
+
+// Components of the kept graph (offs/adj over internal ids; intl maps a
+// vertex's id to its internal id, empty: the same), extended to every vertex
+// through its anchor.  Union-find over the edges in parallel, always linking
+// the larger root under the smaller.
+void label_components(const uint32_t *offs, const uint32_t *adj, uint32_t n, const std::vector<uint32_t> &intl,
+                      TreeInfo &t) {
+    std::vector<uint32_t> root(n);
+    for (uint32_t v = 0; v < n; ++v) root[v] = v;
+    auto find = [&](uint32_t v) {
+        uint32_t r = __atomic_load_n(&root[v], __ATOMIC_RELAXED);
+        while (r != v) {
+            const uint32_t g = __atomic_load_n(&root[r], __ATOMIC_RELAXED);
+            __atomic_compare_exchange_n(&root[v], &r, g, false, __ATOMIC_RELAXED, __ATOMIC_RELAXED);  // halving
+            v = r;
+            r = g;
+        }
+        return v;
+    };
+#pragma omp parallel for schedule(dynamic, 2048)
+    for (int64_t vi = 0; vi < (int64_t)n; ++vi) {
+        const uint32_t v = (uint32_t)vi;
+        for (uint32_t e = offs[v]; e < offs[v + 1]; ++e) {
+            uint32_t a = v, b = adj[e];
+            if (b <= a) continue;  // each edge once (lists are symmetric)
+            for (;;) {
+                a = find(a);
+                b = find(b);
+                if (a == b) break;
+                if (a < b) std::swap(a, b);  // link the larger root a under b
+                uint32_t expect = a;
+                if (__atomic_compare_exchange_n(&root[a], &expect, b, false, __ATOMIC_RELAXED, __ATOMIC_RELAXED))
+                    break;
+            }
+        }
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t v = 0; v < (int64_t)n; ++v) __atomic_store_n(&root[v], find((uint32_t)v), __ATOMIC_RELAXED);
+    // dense component numbers, in the order of each component's first vertex
+    std::vector<uint32_t> id(n, kNoRoot);
+    t.comp.assign(n, kNoRoot);
+    t.comp_n.clear();
+    for (uint32_t v = 0; v < n; ++v) {
+        const uint32_t a = t.anchor[v];
+        const uint32_t r = root[intl.empty() ? a : intl[a]];
+        if (id[r] == kNoRoot) {
+            id[r] = (uint32_t)t.comp_n.size();
+            t.comp_n.push_back(0);
+        }
+        t.comp[v] = id[r];
+        ++t.comp_n[id[r]];
+    }
 }
 
 void tree_bc(const TreeInfo &t, const std::vector<uint32_t> &cnt, std::vector<double> &acc) {

@@ -28,11 +28,12 @@ int main() {
     for (auto &x : adj) scanf("%u", &x);
     for (unsigned i = 0; i < k; ++i) { unsigned s; scanf("%u", &s); if (offs[s + 1] > offs[s]) ++cnt[s]; }
     TreeInfo t;
-    std::vector<uint32_t> co, ca;
-    peel_trees(offs.data(), adj.data(), n, t, co, ca);
+    std::vector<uint32_t> cdeg, ext, intl, o2, a2;
+    peel_trees(offs.data(), adj.data(), n, t, cdeg, ext, intl, o2, a2);
+    label_components(o2.data(), a2.data(), n, intl, t);
     std::vector<double> acc;
     tree_bc(t, cnt, acc);
-    printf("%zu %zu\n", t.order.size(), ca.size());
+    printf("%zu %zu\n", t.order.size(), a2.size());
     for (unsigned v = 0; v < n; ++v) printf("%.17g %u\n", acc[v], t.anchor[v]);
 }
 """
@@ -102,12 +103,11 @@ int main() {
     for (auto &x : offs) scanf("%u", &x);
     for (auto &x : adj) scanf("%u", &x);
     TreeInfo t;
-    std::vector<uint32_t> co, ca, ext, intl, o2, a2;
-    peel_trees(offs.data(), adj.data(), n, t, co, ca);
-    const uint32_t nlive = relabel_live(co, ca, n, ext, intl, o2, a2);
+    std::vector<uint32_t> cdeg, ext, intl, o2, a2;
+    const uint32_t nlive = peel_trees(offs.data(), adj.data(), n, t, cdeg, ext, intl, o2, a2);
     printf("%u\n", nlive);
-    for (auto x : co) printf("%u ", x); printf("\n");
-    for (auto x : ca) printf("%u ", x); printf("\n");
+    for (auto x : t.parent) printf("%u ", x == kNoRoot ? 0u : 1u); printf("\n");
+    for (auto x : cdeg) printf("%u ", x); printf("\n");
     for (auto x : ext) printf("%u ", x); printf("\n");
     for (auto x : o2) printf("%u ", x); printf("\n");
     for (auto x : a2) printf("%u ", x); printf("\n");
@@ -116,8 +116,9 @@ int main() {
 
 
 def test_relabel_keeps_the_kept_graph(tmp_path):
-    """The searched graph is renumbered with its vertices that have edges
-    first, in their original order; the renumbered CSR is the same graph."""
+    """The kept graph (every edge between two unpeeled vertices) comes out
+    renumbered with its vertices that keep an edge first, in their original
+    order; the renumbered CSR is that graph."""
     (tmp_path / "r.cpp").write_text(RELABEL)
     exe = tmp_path / "r"
     subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "ck-bc_b200", "csrc"), "-I",
@@ -129,8 +130,9 @@ def test_relabel_keeps_the_kept_graph(tmp_path):
     txt = f"{n} {len(adj)}\n" + " ".join(map(str, offs)) + "\n" + " ".join(map(str, adj)) + "\n"
     out = subprocess.run([str(exe)], input=txt, capture_output=True, text=True, check=True).stdout.split("\n")
     nlive = int(out[0])
-    co, ca, ext, o2, a2 = (np.array(out[i].split(), dtype=np.int64) for i in range(1, 6))
-    cdeg = np.diff(co)
+    peeled, cdeg, ext, o2, a2 = (np.array(out[i].split(), dtype=np.int64) for i in range(1, 6))
+    kept = [[] if peeled[v] else [u for u in adj[offs[v]:offs[v + 1]] if not peeled[u]] for v in range(n)]
+    assert cdeg.tolist() == [len(k) for k in kept]
     assert nlive == int((cdeg > 0).sum()) and 0 < nlive < n
     assert sorted(ext.tolist()) == list(range(n))
     assert np.all(cdeg[ext[:nlive]] > 0) and np.all(cdeg[ext[nlive:]] == 0)
@@ -139,4 +141,4 @@ def test_relabel_keeps_the_kept_graph(tmp_path):
     intl[ext] = np.arange(n)
     for i in range(n):
         v = ext[i]
-        assert a2[o2[i]:o2[i + 1]].tolist() == intl[ca[co[v]:co[v + 1]]].tolist()
+        assert a2[o2[i]:o2[i + 1]].tolist() == intl[np.array(kept[v], dtype=np.int64)].tolist()
