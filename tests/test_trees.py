@@ -142,3 +142,60 @@ def test_relabel_keeps_the_kept_graph(tmp_path):
     for i in range(n):
         v = ext[i]
         assert a2[o2[i]:o2[i + 1]].tolist() == intl[np.array(kept[v], dtype=np.int64)].tolist()
+
+
+COMPONENTS = r"""
+#include <cstdio>
+#include <vector>
+#include "engine_internal.hpp"
+using namespace bcg;
+int main() {
+    unsigned n, m;
+    if (scanf("%u %u", &n, &m) != 2) return 1;
+    std::vector<uint32_t> offs(n + 1), adj(m);
+    for (auto &x : offs) scanf("%u", &x);
+    for (auto &x : adj) scanf("%u", &x);
+    TreeInfo t;
+    std::vector<uint32_t> cdeg, ext, intl, o2, a2;
+    peel_trees(offs.data(), adj.data(), n, t, cdeg, ext, intl, o2, a2);
+    label_components(o2.data(), a2.data(), n, intl, t);
+    printf("%zu\n", t.comp_n.size());
+    for (auto x : t.comp) printf("%u ", x); printf("\n");
+    for (auto x : t.comp_n) printf("%lu ", (unsigned long)x); printf("\n");
+}
+"""
+
+
+@pytest.mark.parametrize("spec", ["er:scale=14,ef=1,seed=11", "rmat:scale=13,ef=2,seed=4,pendant_frac=0.3,pendant_mean=6"])
+def test_parallel_components_match_scipy(tmp_path, spec):
+    """Peeling and the union-find component labels, built with OpenMP and run
+    on 8 threads, against scipy's connected components of the input graph:
+    the same partition, numbered in the order of each component's first
+    vertex, with the right sizes."""
+    scipy_cc = pytest.importorskip("scipy.sparse.csgraph")
+    import scipy.sparse as sp
+    (tmp_path / "c.cpp").write_text(COMPONENTS)
+    exe = tmp_path / "c"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-fopenmp", "-I", os.path.join(ROOT, "ck-bc_b200", "csrc"), "-I",
+                    os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include",
+                    os.path.join(ROOT, "ck-bc_b200", "csrc", "trees.cpp"), str(tmp_path / "c.cpp"), "-o", str(exe)],
+                   check=True)
+    offs, adj = bcg.generate(spec)
+    n = len(offs) - 1
+    txt = f"{n} {len(adj)}\n" + " ".join(map(str, offs)) + "\n" + " ".join(map(str, adj)) + "\n"
+    env = dict(os.environ, OMP_NUM_THREADS="8")
+    for _ in range(3):  # thread interleavings differ from run to run
+        out = subprocess.run([str(exe)], input=txt, capture_output=True, text=True, check=True, env=env).stdout.split("\n")
+        ncomp = int(out[0])
+        comp = np.array(out[1].split(), dtype=np.int64)
+        comp_n = np.array(out[2].split(), dtype=np.int64)
+        g = sp.csr_matrix((np.ones(len(adj)), adj.astype(np.int64), offs.astype(np.int64)), shape=(n, n))
+        nref, lab = scipy_cc.connected_components(g, directed=False)
+        assert ncomp == nref
+        # renumber scipy's labels by first vertex, as the harness does
+        first = {}
+        for v in range(n):
+            first.setdefault(lab[v], len(first))
+        ref = np.array([first[x] for x in lab])
+        assert np.array_equal(comp, ref)
+        assert np.array_equal(comp_n, np.bincount(ref, minlength=nref))
