@@ -746,7 +746,7 @@ static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint3
         g->h_intl = std::move(intl);
         g->h_lab_offs = std::move(lab_offs);
         g->h_lab_adj = std::move(lab_adj);
-        g->comp_job = std::async(std::launch::async, [g]() {
+        auto job = [g]() {
             try {
                 label_components(g->h_lab_offs.data(), g->h_lab_adj.data(), g->n, g->h_intl, g->tinfo);
             } catch (...) {
@@ -755,7 +755,12 @@ static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint3
             std::vector<uint32_t>().swap(g->h_lab_offs);
             std::vector<uint32_t>().swap(g->h_lab_adj);
             return (int)BCG_OK;
-        });
+        };
+        try {
+            g->comp_job = std::async(std::launch::async, job);
+        } catch (...) {  // no thread to be had: label them now
+            if (job() != BCG_OK) return fail(set_error(BCG_ERR_OOM, "labelling the components: out of host memory"));
+        }
     }
     *out = g;
     return BCG_OK;
