@@ -10,8 +10,10 @@ no public dataset is involved.
 A step = one exact-BC pass over the step's sources (one kernel launch of the
 engine), preceded (untimed) by a reset of the bc accumulator and an L2 flush
 (a 512 MiB device write, larger than the 126 MB L2).  With N ranks (one per
-GPU, torchrun) every rank takes its own block of 4096 sources (weak scaling)
-and the step ends with an NCCL all-reduce of the FP64 bc vector.
+GPU; `--gpus N` starts them itself through torch.distributed.run when no
+launcher did) every rank takes its own block of 4096 sources (weak scaling)
+and the step ends with the path's one exchange: the FP64 bc partials
+all-gathered over NCCL and added in rank order (bit-reproducible).
 
   value  TEPS = sum over all ranks' sources of the undirected edge count of
          the source's component / max-over-ranks device time (CUDA events on
@@ -26,7 +28,8 @@ and the step ends with an NCCL all-reduce of the FP64 bc vector.
          bounded sample of the same workload's sources, rank 0 at N=1.
 --impl reference: the reference program has no CPU Brandes; its path is timed
 through the oracle port on the host cores (all threads), each step a bounded
-sample of the same sources.
+sample of the same sources, on the same graph rebuilt by oracle/graphgen.py
+(no product library is loaded by that arm).
 """
 from __future__ import annotations
 
@@ -135,6 +138,41 @@ def traffic_per_source(prune: str):
         return None, ""
 
 
+def rank_sources(sampler, n, per_rank, rank, world):
+    """This rank's block of the workload's sources: per_rank * world distinct
+    sources drawn with the workload's seed, cut into contiguous blocks in rank
+    order (weak scaling: every rank runs per_rank sources)."""
+    sys.path.insert(0, os.path.join(ROOT, "ck-bc_b200"))
+    import shard
+
+    return shard.shard_sources(sampler(n, per_rank * world, SRC_SEED), rank, world)
+
+
+def combine_bc(bc_t):
+    """The step's one exchange: every rank's FP64 bc partial summed in rank
+    order (all-gather, then a fixed-order add), so the result is the same
+    bits on every run and every rank."""
+    import shard
+
+    return shard.reduce_bc(bc_t, deterministic=True)
+
+
+def relaunch(args):
+    """--gpus N > 1 without a launcher: start N ranks of this script with
+    torch.distributed.run (one per GPU, rendezvous on 127.0.0.1) and return
+    its exit code; rank 0 prints the JSON line."""
+    import socket
+
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = ["timeout", "-k", "60", "3600", sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={args.gpus}", "--master-addr=127.0.0.1", f"--master-port={port}",
+           os.path.abspath(__file__)] + sys.argv[1:]
+    log(f"starting {args.gpus} ranks: {' '.join(cmd[4:])}")
+    return subprocess.call(cmd)
+
+
 def cpu_baseline(offs, adj, sources, budget_s=15.0):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
@@ -152,21 +190,26 @@ def cpu_baseline(offs, adj, sources, budget_s=15.0):
         done += len(s)
     el = time.perf_counter() - t0
     return {"value": edges / el if el > 0 else None, "unit": "TEPS", "cores": nt, "kind": "port",
-            "sample": f"first {done} of the {len(sources)} workload sources, oracle/brandes.c FP64 Brandes, "
-                      f"{nt} OpenMP threads, {el:.1f} s"}
+            "sample": f"first {done} of the {len(sources)} workload sources, oracle/brandes.c FP64 Brandes on the "
+                      f"unpruned graph (no pendant folding), {nt} OpenMP threads, {el:.1f} s"}
 
 
 def run_reference(args, rank, world):
-    """--impl reference: the reference path's CPU restatement, all host threads."""
+    """--impl reference: the reference path's CPU restatement, all host threads.
+    The graph and sources come from oracle/graphgen.py (the seeded generators
+    restated in numpy, bit-identical to the library's), so this arm loads
+    only oracle/ code."""
     if rank != 0:
         return 0
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import bcg
+    import graphgen
     import oracle
 
-    offs, adj = bcg.generate(SPEC)
+    t_gen = time.perf_counter()
+    offs, adj = graphgen.generate(args.graph)
     n = len(offs) - 1
-    srcs = bcg.sample_sources(n, NSRC, SRC_SEED)
+    srcs = rank_sources(graphgen.sample_sources, n, args.sources, 0, 1)
+    log(f"[reference] graph n={n} nnz={len(adj)} generated in {time.perf_counter() - t_gen:.1f}s (numpy)")
     nt = oracle.max_threads()
     per_step = max(nt, 1)
     times, edges = [], []
@@ -185,11 +228,13 @@ def run_reference(args, rank, world):
     out = {"metric": METRIC, "value": val, "unit": "TEPS", "impl": "reference", "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / max(1, len(times)),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": WORKLOAD, "graph": SPEC, "sources": NSRC, "source_seed": SRC_SEED,
+           "config": {"workload": WORKLOAD, "graph": args.graph, "n": n, "m": len(adj) // 2,
+                      "sources_per_gpu": args.sources, "source_seed": SRC_SEED, "pruning": "none",
                       "sample_per_step": per_step},
            "cpu_baseline": {"value": val, "unit": "TEPS", "cores": nt, "kind": "port",
-                            "sample": f"{per_step} sources per step of the workload's 4096, oracle/brandes.c "
-                                      f"(the reference has no CPU Brandes), {nt} OpenMP threads"},
+                            "sample": f"{per_step} sources per step of the workload's {args.sources}, "
+                                      f"oracle/brandes.c FP64 Brandes on the unpruned graph (no pendant "
+                                      f"folding; the reference has no CPU Brandes), {nt} OpenMP threads"},
            "e2e": {"value": val, "unit": "TEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
     return 0
@@ -502,8 +547,11 @@ def main():
     ap.add_argument("--prune", default="trees", choices=["degree1", "trees"],
                     help="plain/grid forms: whole pendant trees (default) or one layer of degree-1 vertices "
                          "(as bc2d -H 1)")
+    ap.add_argument("--graph", default=SPEC, help="plain form: generator spec (default: the workload's graph)")
     args = ap.parse_args()
 
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return relaunch(args)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -536,11 +584,10 @@ def main():
         torch.cuda.synchronize()
 
     t_gen = time.perf_counter()
-    offs, adj = bcg.generate(SPEC)
+    offs, adj = bcg.generate(args.graph)
     n = len(offs) - 1
     ns = args.sources
-    all_src = bcg.sample_sources(n, ns * world, SRC_SEED)
-    srcs = np.ascontiguousarray(all_src[rank * ns:(rank + 1) * ns])
+    srcs = rank_sources(bcg.sample_sources, n, ns, rank, world)
     log(f"[rank {rank}] graph n={n} nnz={len(adj)} generated in {time.perf_counter() - t_gen:.1f}s")
 
     pflag = bcg.PRUNE_TREES if args.prune == "trees" else bcg.PRUNE_DEGREE1
@@ -560,7 +607,7 @@ def main():
         ev0.record(stream)
         st = g.run(srcs)
         if dist is not None:
-            dist.all_reduce(bc_t)
+            combine_bc(bc_t)
         ev1.record(stream)
         torch.cuda.synchronize()
         return ev0.elapsed_time(ev1), st
@@ -570,7 +617,7 @@ def main():
     barrier()
     clocks = ClockSampler(local)
     clocks.start()
-    step_ms, kern_ms, edges, cverts, ran = [], [], 0, 0, 0
+    step_ms, kern_ms, edges, cverts, ran, s_edges, s_verts, roots = [], [], 0, 0, 0, 0, 0, 0
     for _ in range(args.steps):
         ms, st = one_step()
         step_ms.append(ms)
@@ -578,6 +625,9 @@ def main():
         edges += st.teps_edges
         cverts += st.comp_vertices
         ran += st.sources - st.skipped
+        s_edges += st.search_edges
+        s_verts += st.visited
+        roots += st.roots
     clk = clocks.stop()
     barrier()
     tot_ms = sum(step_ms)
@@ -598,9 +648,16 @@ def main():
     achieved = alg_bytes / kern_s / 1e9
     tps, tnote = traffic_per_source(args.prune)
     traffic = tps * (ran / args.steps) if tps is not None else None
+    # the same bytes per search over the graph the kernel actually walks (the
+    # pruned graph, one search per root however many sources it stands for)
+    s_bytes = 16.0 * s_edges + 56.0 * s_verts + 8.0 * roots
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": peak_kind, "traffic": traffic,
-                "alg_bytes_per_launch": alg_bytes / args.steps, "kernel_ms_per_launch": 1e3 * kern_s / args.steps}
+                "alg_bytes_per_launch": alg_bytes / args.steps, "kernel_ms_per_launch": 1e3 * kern_s / args.steps,
+                "searched": {"achieved": s_bytes / kern_s / 1e9, "frac": s_bytes / kern_s / 1e9 / peak,
+                             "bytes_per_launch": s_bytes / args.steps,
+                             "note": "16 B per searched edge + 56 B per searched vertex + 8 B per root, over the "
+                                     "pruned graph each root's search walks"}}
     if tnote:
         roofline["traffic_note"] = tnote
 
@@ -621,7 +678,7 @@ def main():
         st = ge.run(srcs)
         if dist is not None:
             bt = torch.as_tensor(bcg.DeviceArray(ge.bc_device_ptr(), n), device="cuda")
-            dist.all_reduce(bt)
+            combine_bc(bt)
         t2 = time.perf_counter()
         bcg.lib().bcg_get_bc(ge.h, h_bc.ctypes.data_as(bcg._f64p))
         torch.cuda.synchronize()
@@ -652,11 +709,12 @@ def main():
         out = {"metric": METRIC, "value": value, "unit": "TEPS", "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-               "config": {"workload": WORKLOAD, "graph": SPEC, "n": n, "m": len(adj) // 2,
+               "config": {"workload": WORKLOAD, "graph": args.graph, "n": n, "m": len(adj) // 2,
                           "sources_per_gpu": ns, "source_seed": SRC_SEED,
                           "pruning": "pendant trees" if args.prune == "trees" else "degree-1",
                           "sources_skipped_per_step": int(st.skipped), "batch_width": int(st.batch_width),
-                          "parallelism": f"source-sharded x{world}" if world > 1 else "1 GPU",
+                          "parallelism": f"source-sharded x{world}, bc summed in rank order" if world > 1
+                          else "1 GPU",
                           "l2": "512 MiB flush write between steps (untimed); graph + state exceed L2"},
                "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clk,
                "gpu_launches": args.steps}

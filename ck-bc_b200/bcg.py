@@ -56,7 +56,8 @@ class Stats(ctypes.Structure):
                 ("teps_edges", ctypes.c_uint64), ("visited", ctypes.c_uint64),
                 ("comp_vertices", ctypes.c_uint64),
                 ("max_depth", ctypes.c_uint32), ("batch_width", ctypes.c_uint32),
-                ("kernel_ms", ctypes.c_double), ("extended_sigma", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("kernel_ms", ctypes.c_double), ("extended_sigma", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("search_edges", ctypes.c_uint64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -96,6 +97,8 @@ SIGNATURES = {
     "bcg_bc_csr": (ctypes.c_int, [_u32p, _u32p, ctypes.c_uint32, ctypes.c_uint64, _u32p, ctypes.c_uint64,
                                   ctypes.c_uint32, _f64p, ctypes.POINTER(Stats)]),
     "bcg_single_source": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, _i32p, _u64p, _f64p]),
+    "bcg_debug_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, _u32p, ctypes.c_uint32, _i32p, _u64p,
+                                       _f64p]),
     "bcg_graph_pruning": (ctypes.c_int, [ctypes.c_void_p, _u32p, _u32p]),
     "bcg_graph_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32),
                                       ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
@@ -291,6 +294,18 @@ class Graph:
         dl = np.zeros(self.n, dtype=np.float64)
         _check(lib().bcg_single_source(self.h, src, lvl.ctypes.data_as(_i32p), sig.ctypes.data_as(_u64p),
                                        dl.ctypes.data_as(_f64p)))
+        return lvl, sig, dl
+
+    def debug_batch(self, roots, width: int):
+        """One real batch of `width` slots with roots[k] in slot k -> (level,
+        sigma, delta), each of shape (len(roots), n) in the caller's ids."""
+        r = np.ascontiguousarray(roots, dtype=np.uint32)
+        k = len(r)
+        lvl = np.zeros((k, self.n), dtype=np.int32)
+        sig = np.zeros((k, self.n), dtype=np.uint64)
+        dl = np.zeros((k, self.n), dtype=np.float64)
+        _check(lib().bcg_debug_batch(self.h, width, _p32(r), k, lvl.ctypes.data_as(_i32p), sig.ctypes.data_as(_u64p),
+                                     dl.ctypes.data_as(_f64p)))
         return lvl, sig, dl
 
     def pruning(self):

@@ -110,14 +110,6 @@ __global__ void k_vinfo_plain(uint32_t n, const uint32_t *__restrict__ offs, uin
     if (v < n) vinfo[v] = make_uint2(offs[v + 1] - offs[v], 0u);
 }
 
-// Levels of slot 0 of a single-slot run (rows of row_bytes(1) bytes, level first).
-__global__ void k_levels_out(uint32_t n, const unsigned char *__restrict__ rows, int32_t *__restrict__ out) {
-    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= n) return;
-    const uint16_t l = *reinterpret_cast<const uint16_t *>(rows + (size_t)v * row_bytes(1));
-    out[v] = l == kUnvisited ? -1 : (int32_t)l;
-}
-
 // ---------------------------------------------------------------------------
 // Work tiles (host, from the original row starts).
 // ---------------------------------------------------------------------------
@@ -131,11 +123,12 @@ __global__ void k_levels_out(uint32_t n, const unsigned char *__restrict__ rows,
 // kHubFlag, when v is split).
 static void build_tiles(const uint32_t *offs, uint32_t n, uint32_t tn, uint32_t vcap, uint32_t ecap,
                         const std::vector<uint32_t> &breaks, std::vector<Tile> &tiles, uint32_t &nhub,
-                        std::vector<uint32_t> &tile_of) {
+                        uint32_t &nhubchunks, std::vector<uint32_t> &tile_of) {
     tiles.clear();
     tile_of.assign(n, 0);  // vertices past tn (no edges: never reached) keep tile 0
     n = tn;
     nhub = 0;
+    nhubchunks = 0;
     uint32_t v = 0;
     size_t nb = 0;  // next break point
     while (v < n) {
@@ -152,6 +145,8 @@ static void build_tiles(const uint32_t *offs, uint32_t n, uint32_t tn, uint32_t 
                 t.e1 = std::min(offs[v + 1], t.e0 + ecap);
                 t.hub = (int32_t)nhub;
                 t.nchunks = nch;
+                t.hslot = nhubchunks++;
+                t.hchunk = c;
                 tiles.push_back(t);
             }
             ++nhub;
@@ -211,8 +206,8 @@ int ensure_state(bcg_graph *g, uint32_t S) {
     cudaFree(g->d_lists); g->d_lists = nullptr;
     g->state_width = 0;
     CK(cudaMalloc(&g->d_rows, (size_t)g->n * row_bytes((int)S)));
-    CK(cudaMalloc(&g->d_hub_acc, (size_t)std::max(1u, g->nhub) * S * sizeof(unsigned long long)));
-    CK(cudaMemset(g->d_hub_acc, 0, (size_t)std::max(1u, g->nhub) * S * sizeof(unsigned long long)));
+    // one slot per hub chunk, written by the chunk before it is read
+    CK(cudaMalloc(&g->d_hub_acc, (size_t)std::max(1u, g->nhubchunks) * S * sizeof(unsigned long long)));
     // every (tile, level) pair is listed at most once per batch: a tile is on
     // level d's list only if one of its vertices (or chunks) first reaches d,
     // so the lists of one batch hold at most S * (n + ntiles) entries
@@ -260,7 +255,7 @@ static int setup_tiles(bcg_graph *g, const uint32_t *h_offs) {
     std::vector<Tile> tiles;
     std::vector<uint32_t> tile_of;
     build_tiles(h_offs, n, g->tile_n ? g->tile_n : n, g->tile_vcap, g->tile_ecap, g->tile_breaks, tiles, g->nhub,
-                tile_of);
+                g->nhubchunks, tile_of);
     g->ntiles = (uint32_t)tiles.size();
     CK(cudaMalloc(&g->d_tiles, std::max<size_t>(1, tiles.size()) * sizeof(Tile)));
     if (!tiles.empty())
@@ -276,7 +271,9 @@ static int setup_tiles(bcg_graph *g, const uint32_t *h_offs) {
 
 static int create_common(bcg_graph *g, const uint32_t *h_offs) {
     const uint32_t n = g->n;
-    CK(cudaMalloc(&g->d_vinfo, (size_t)n * sizeof(uint2)));
+    // 4 entries of tail padding (the sweep copies 16-byte aligned ranges)
+    CK(cudaMalloc(&g->d_vinfo, ((size_t)n + 4) * sizeof(uint2)));
+    CK(cudaMemset(g->d_vinfo, 0, ((size_t)n + 4) * sizeof(uint2)));
     CK(cudaMalloc(&g->d_bc, (size_t)n * sizeof(double)));
     CK(cudaMemset(g->d_bc, 0, (size_t)n * sizeof(double)));
     CK(cudaMalloc(&g->d_ctrl, sizeof(Ctrl)));
@@ -374,8 +371,10 @@ __global__ void k_add(uint32_t n, double *__restrict__ bc, const double *__restr
 // terms) for this run's sources, added on the device after the search.
 static int add_tree_terms(bcg_graph *g, const uint32_t *src, uint64_t nsrc, const RunPlan &p, cudaStream_t st,
                           bcg_stats *stats) {
-    if (g->comp_job.valid() && g->comp_job.get() != BCG_OK)
-        return set_error(BCG_ERR_OOM, "labelling the components: out of host memory");
+    // the labelling job's outcome is kept: a failed job fails this run and
+    // every later one (its labels are incomplete)
+    if (g->comp_job.valid()) g->comp_rc = g->comp_job.get();
+    if (g->comp_rc != BCG_OK) return set_error(BCG_ERR_OOM, "labelling the components: out of host memory");
     std::vector<uint32_t> cnt(g->n, 0);
     for (uint64_t i = 0; i < nsrc; ++i)
         if (g->h_deg[src[i]]) ++cnt[src[i]];
@@ -453,15 +452,23 @@ static void fill_args(bcg_graph *g, BatchArgs &a) {
     a.directed = (g->flags & BCG_DIRECTED) ? 1 : 0;
 }
 
-static int run_plan(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *stats, bool debug,
-                    unsigned long long *dbg_sigma, double *dbg_delta) {
+// Debug outputs of a single-batch run (internal numbering, slot-major).
+struct DebugOut {
+    uint32_t width = 0;  // 0: not a debug run
+    int32_t *level = nullptr;
+    unsigned long long *sigma = nullptr;
+    double *delta = nullptr;
+};
+
+static int run_plan(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *stats, const DebugOut &dbg) {
+    const bool debug = dbg.width != 0;
     const uint64_t nroots = p.roots.size();
     if (stats) {
         stats->skipped = p.skipped;
         stats->roots = nroots;
     }
     if (nroots == 0) return BCG_OK;
-    const uint32_t S = debug ? 1u : choose_width(g, nroots);
+    const uint32_t S = debug ? dbg.width : choose_width(g, nroots);
     int rc = ensure_state(g, S);
     if (rc) return rc;
     const uint64_t nbatch = (nroots + S - 1) / S;
@@ -474,12 +481,11 @@ static int run_plan(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *
     CK(cudaMemcpyAsync(g->d_roots, roots.data(), slots * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(g->d_pend, pend.data(), slots * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(g->d_mult, mult.data(), slots * sizeof(double), cudaMemcpyHostToDevice, st));
-    CK(cudaMemsetAsync(g->d_hub_acc, 0, (size_t)std::max(1u, g->nhub) * g->state_width * sizeof(unsigned long long), st));
-    CK(cudaMemsetAsync(g->d_hub_cnt, 0, (size_t)std::max(1u, g->nhub) * sizeof(unsigned int), st));
     BatchArgs a{};
     fill_args(g, a);
-    a.dbg_sigma = dbg_sigma;
-    a.dbg_delta = dbg_delta;
+    a.dbg_level = dbg.level;
+    a.dbg_sigma = dbg.sigma;
+    a.dbg_delta = dbg.delta;
     // optional per-sweep trace: BCG_TRACE_FILE=<path> appends one CSV line per
     // sweep (batch, kind, level, tiles walked, pairs discovered, end time)
     const char *trace_path = getenv("BCG_TRACE_FILE");
@@ -514,6 +520,7 @@ static int run_plan(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *
             CK(cudaMemcpyAsync(&g->d_ctrl->wait_ns, &g->wait_ns, sizeof(unsigned long long), cudaMemcpyHostToDevice,
                                st));
             CK(cudaMemsetAsync(g->d_tmark, 0, (size_t)std::max(1u, g->ntiles) * sizeof(uint32_t), st));
+            CK(cudaMemsetAsync(g->d_hub_cnt, 0, (size_t)std::max(1u, g->nhub) * sizeof(unsigned int), st));
             a.roots = g->d_roots + b0 * S;
             a.mult = g->d_mult + b0 * S;
             a.pend = g->d_pend + b0 * S;
@@ -574,12 +581,15 @@ static int run_plan(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *
     if (stats) {
         std::vector<RootStat> rs(slots);
         CK(cudaMemcpy(rs.data(), g->d_rstat, slots * sizeof(RootStat), cudaMemcpyDeviceToHost));
-        uint64_t teps = 0, vis = 0, cv = 0;
+        uint64_t teps = 0, vis = 0, cv = 0, se = 0;
         uint32_t md = 0;
         for (uint64_t i = 0; i < nroots; ++i) {
             teps += p.count[i] * (rs[i].mc2 / 2);
             cv += p.count[i] * rs[i].wsum;
             vis += rs[i].visited;
+            // mc2 = sum of (deg + 2 reach) and wsum = sum of (1 + reach) over
+            // the visited vertices: the searched degrees sum to mc2 - 2 (wsum - visited)
+            se += (rs[i].mc2 - 2 * (rs[i].wsum - rs[i].visited)) / 2;
             md = std::max(md, rs[i].depth);
         }
         float ms = 0.f;
@@ -592,6 +602,7 @@ static int run_plan(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *
         stats->batch_width = S;
         stats->kernel_ms = ms;
         stats->extended_sigma = ext ? 1u : 0u;
+        stats->search_edges = se;
     }
     return BCG_OK;
 }
@@ -603,7 +614,6 @@ int enqueue_packed(bcg_graph *g, const PackedRun &p, uint32_t S, cudaStream_t st
     int rc = ensure_state(g, S);
     if (rc) return rc;
     const size_t nh = std::max(1u, g->nhub);
-    CK(cudaMemsetAsync(g->d_hub_acc, 0, nh * S * sizeof(unsigned long long), st));
     CK(cudaMemsetAsync(g->d_hub_cnt, 0, nh * sizeof(unsigned int), st));
     CK(cudaMemsetAsync(g->d_ctrl, 0, sizeof(Ctrl), st));  // wait bound 0: the kernel's default
     CK(cudaMemsetAsync(g->d_tmark, 0, (size_t)std::max(1u, g->ntiles) * sizeof(uint32_t), st));
@@ -711,13 +721,15 @@ static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint3
     if (trees) g->tile_n = nlive ? nlive : 1;
     auto fail = [&](int code) { graph_free(g); return code; };
     cudaError_t e;
-    if ((e = cudaMalloc(&g->d_offs, ((size_t)n + 1) * sizeof(uint32_t))) != cudaSuccess ||
-        // 4 entries of tail padding: the sweep copies adjacency ranges in
-        // 16-byte aligned chunks that may end up to 12 bytes past nnz
+    // 4 entries of tail padding on offsets and adjacency: the sweep copies
+    // their ranges in 16-byte aligned pieces that may end up to 12 bytes
+    // past the last entry
+    if ((e = cudaMalloc(&g->d_offs, ((size_t)n + 1 + 4) * sizeof(uint32_t))) != cudaSuccess ||
         (e = cudaMalloc(&g->d_adj, (dev_nnz + 4) * sizeof(uint32_t))) != cudaSuccess)
         return fail(set_error(BCG_ERR_OOM, "cudaMalloc CSR: %s", cudaGetErrorString(e)));
     const cudaMemcpyKind kind = device_in ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     if ((e = cudaMemcpy(g->d_offs, offsets, ((size_t)n + 1) * sizeof(uint32_t), kind)) != cudaSuccess ||
+        (e = cudaMemset(g->d_offs + n + 1, 0, 4 * sizeof(uint32_t))) != cudaSuccess ||
         (dev_nnz && (e = cudaMemcpy(g->d_adj, adj, dev_nnz * sizeof(uint32_t), kind)) != cudaSuccess) ||
         (e = cudaMemset(g->d_adj + dev_nnz, 0, 4 * sizeof(uint32_t))) != cudaSuccess)
         return fail(set_error(BCG_ERR_CUDA, "uploading CSR: %s", cudaGetErrorString(e)));
@@ -800,7 +812,7 @@ int bcg_run(bcg_graph *g, const uint32_t *sources, uint64_t nsrc, bcg_stats *sta
     RunPlan p;
     int rc = plan_run(g, sources, nsrc, p);
     if (rc) return rc;
-    rc = run_plan(g, p, 0, st, false, nullptr, nullptr);
+    rc = run_plan(g, p, 0, st, DebugOut{});
     if (rc || !g->trees) return rc;
     return add_tree_terms(g, sources, nsrc, p, 0, st);
 }
@@ -818,7 +830,7 @@ int bcg_run_device(bcg_graph *g, const uint32_t *d_sources, uint64_t nsrc, void 
     RunPlan p;
     int rc = plan_run(g, h.data(), nsrc, p);
     if (rc) return rc;
-    rc = run_plan(g, p, st, stats, false, nullptr, nullptr);
+    rc = run_plan(g, p, st, stats, DebugOut{});
     if (rc || !g->trees) return rc;
     return add_tree_terms(g, h.data(), nsrc, p, st, stats);
 }
@@ -850,54 +862,92 @@ int bcg_bc_csr(const uint32_t *offsets, const uint32_t *adj, uint32_t n, uint64_
     return rc;
 }
 
-static int single_source_impl(bcg_graph *g, uint32_t src, int32_t *level, uint64_t *sigma, double *delta) {
-    if (g->trees) return set_error(BCG_ERR_ARG, "single-source runs are not available with BCG_PRUNE_TREES");
-    clear_error();
-    if (!g) return set_error(BCG_ERR_ARG, "null handle");
-    if (src >= g->n) return set_error(BCG_ERR_ARG, "source %u >= n=%u", src, g->n);
+// One batch of up to `width` roots (caller's ids) run in debug mode: every
+// slot's levels and sigma after the forward pass and delta after the
+// backward pass, copied out slot-major in the caller's numbering (nroots * n
+// values each; vertices the search does not hold, i.e. pendant-tree
+// vertices in BCG_PRUNE_TREES mode, read level -1, sigma 0, delta 0).  The bc
+// accumulator is saved and restored around the run.
+static int debug_batch_impl(bcg_graph *g, uint32_t width, const uint32_t *roots, uint32_t nroots, int32_t *level,
+                            uint64_t *sigma, double *delta) {
+    if (!g || (nroots && !roots)) return set_error(BCG_ERR_ARG, "null argument");
+    if (width != 1 && width != 3 && width != 6) return set_error(BCG_ERR_ARG, "batch width %u not in {1,3,6}", width);
+    if (nroots == 0 || nroots > width) return set_error(BCG_ERR_ARG, "%u roots for a batch of width %u", nroots, width);
     const size_t n = g->n;
-    // the bc accumulator is saved and restored around the run
+    const size_t ns = g->tile_n ? g->tile_n : g->n;  // searched vertices (the kernel's stride)
+    RunPlan p;
+    for (uint32_t k = 0; k < nroots; ++k) {
+        const uint32_t r = roots[k];
+        if (r >= g->n) return set_error(BCG_ERR_ARG, "root %u >= n=%u", r, g->n);
+        const uint32_t ri = g->h_intl.empty() ? r : g->h_intl[r];
+        if (g->trees && (g->h_cdeg[r] == 0 || ri >= ns))
+            return set_error(BCG_ERR_ARG, "root %u is not searched: it lies in a pendant tree or has no kept edge", r);
+        p.roots.push_back(ri);
+        p.pend.push_back(0);
+        p.mult.push_back(1.0);
+        p.count.push_back(1);
+    }
+    const size_t cells = ns * width;
     double *d_save = nullptr;
     unsigned long long *d_sig = nullptr;
     double *d_del = nullptr;
     int32_t *d_lvl = nullptr;
-    int rc = BCG_OK;
     auto cleanup = [&]() { cudaFree(d_save); cudaFree(d_sig); cudaFree(d_del); cudaFree(d_lvl); };
     if (cudaMalloc(&d_save, n * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&d_sig, n * sizeof(unsigned long long)) != cudaSuccess ||
-        cudaMalloc(&d_del, n * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&d_lvl, n * sizeof(int32_t)) != cudaSuccess) {
+        cudaMalloc(&d_sig, cells * sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc(&d_del, cells * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&d_lvl, cells * sizeof(int32_t)) != cudaSuccess) {
         cleanup();
-        return set_error(BCG_ERR_OOM, "single-source scratch allocation failed");
+        return set_error(BCG_ERR_OOM, "debug-batch scratch allocation failed");
     }
-    cudaMemcpy(d_save, g->d_bc, n * sizeof(double), cudaMemcpyDeviceToDevice);
-    cudaMemset(d_sig, 0, n * sizeof(unsigned long long));
-    cudaMemset(d_del, 0, n * sizeof(double));
-    RunPlan p;
-    p.roots.push_back(src);
-    p.pend.push_back(0);
-    p.mult.push_back(1.0);
-    p.count.push_back(1);
-    rc = run_plan(g, p, 0, nullptr, true, d_sig, d_del);
+    int rc = BCG_OK;
+    if (cudaMemcpy(d_save, g->d_bc, n * sizeof(double), cudaMemcpyDeviceToDevice) != cudaSuccess ||
+        cudaMemset(d_del, 0, cells * sizeof(double)) != cudaSuccess) {
+        cleanup();
+        return set_error(BCG_ERR_CUDA, "debug-batch setup failed");
+    }
+    DebugOut dbg;
+    dbg.width = width;
+    dbg.level = d_lvl;
+    dbg.sigma = d_sig;
+    dbg.delta = d_del;
+    rc = run_plan(g, p, 0, nullptr, dbg);
+    std::vector<int32_t> hl;
+    std::vector<unsigned long long> hs;
+    std::vector<double> hd;
     if (!rc) {
-        k_levels_out<<<(unsigned)((n + 255) / 256), 256>>>(g->n, g->d_rows, d_lvl);
-        cudaError_t e = cudaDeviceSynchronize();
-        if (e != cudaSuccess) rc = set_error(BCG_ERR_CUDA, "levels: %s", cudaGetErrorString(e));
-    }
-    if (!rc && level) cudaMemcpy(level, d_lvl, n * sizeof(int32_t), cudaMemcpyDeviceToHost);
-    if (!rc && sigma) cudaMemcpy(sigma, d_sig, n * sizeof(uint64_t), cudaMemcpyDeviceToHost);
-    if (!rc && delta) {
-        cudaMemcpy(delta, d_del, n * sizeof(double), cudaMemcpyDeviceToHost);
-        // unreachable vertices: delta 0
-        if (level)
-            for (size_t v = 0; v < n; ++v) if (level[v] < 0) delta[v] = 0.0;
+        hl.resize(cells);
+        hs.resize(cells);
+        hd.resize(cells);
+        if (cudaMemcpy(hl.data(), d_lvl, cells * sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(hs.data(), d_sig, cells * sizeof(unsigned long long), cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(hd.data(), d_del, cells * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = set_error(BCG_ERR_CUDA, "reading the debug outputs failed");
     }
     cudaMemcpy(g->d_bc, d_save, n * sizeof(double), cudaMemcpyDeviceToDevice);
     cleanup();
-    return rc;
+    if (rc) return rc;
+    for (uint32_t k = 0; k < nroots; ++k) {
+        for (size_t v = 0; v < n; ++v) {
+            const size_t vi = g->h_intl.empty() ? v : g->h_intl[v];
+            const bool held = vi < ns;
+            const int32_t L = held ? hl[k * ns + vi] : -1;
+            if (level) level[k * n + v] = L;
+            if (sigma) sigma[k * n + v] = (held && L >= 0) ? hs[k * ns + vi] : 0ull;
+            if (delta) delta[k * n + v] = (held && L >= 0) ? hd[k * ns + vi] : 0.0;
+        }
+    }
+    return BCG_OK;
+}
+
+static int single_source_impl(bcg_graph *g, uint32_t src, int32_t *level, uint64_t *sigma, double *delta) {
+    if (g->trees) return set_error(BCG_ERR_ARG, "single-source runs are not available with BCG_PRUNE_TREES");
+    if (src >= g->n) return set_error(BCG_ERR_ARG, "source %u >= n=%u", src, g->n);
+    return debug_batch_impl(g, 1, &src, 1, level, sigma, delta);
 }
 
 int bcg_single_source(bcg_graph *g, uint32_t src, int32_t *level, uint64_t *sigma, double *delta) {
+    clear_error();
     if (!g) return set_error(BCG_ERR_ARG, "null handle");
     const int mode = g->sigma_mode;
     g->sigma_mode = 1;  // uint64 counts: an overflow is an error here
@@ -907,10 +957,22 @@ int bcg_single_source(bcg_graph *g, uint32_t src, int32_t *level, uint64_t *sigm
 }
 
 int bcg_single_source_ext(bcg_graph *g, uint32_t src, int32_t *level, uint64_t *sigma_ext, double *delta) {
+    clear_error();
     if (!g) return set_error(BCG_ERR_ARG, "null handle");
     const int mode = g->sigma_mode;
     g->sigma_mode = 2;
     const int rc = single_source_impl(g, src, level, sigma_ext, delta);
+    g->sigma_mode = mode;
+    return rc;
+}
+
+int bcg_debug_batch(bcg_graph *g, uint32_t width, const uint32_t *roots, uint32_t nroots, int32_t *level,
+                    uint64_t *sigma, double *delta) {
+    clear_error();
+    if (!g) return set_error(BCG_ERR_ARG, "null handle");
+    const int mode = g->sigma_mode;
+    g->sigma_mode = 1;
+    const int rc = debug_batch_impl(g, width, roots, nroots, level, sigma, delta);
     g->sigma_mode = mode;
     return rc;
 }
@@ -977,7 +1039,7 @@ int bcg_run_weighted(bcg_graph *g, const uint32_t *roots, const double *mult, co
         p.pend.push_back(pend ? pend[i] : 0u);
         p.count.push_back(1);
     }
-    return run_plan(g, p, 0, st, false, nullptr, nullptr);
+    return run_plan(g, p, 0, st, DebugOut{});
 }
 
 int bcg_set_batch_width(bcg_graph *g, uint32_t width) {

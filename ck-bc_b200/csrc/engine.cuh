@@ -5,12 +5,11 @@
 
 namespace bcg {
 
-// Sweep kernel geometry (one CTA per SM; the build may override both).
+// Sweep kernel geometry (one CTA per SM; the build may override both).  256
+// threads: each lane keeps the rows of a whole run (8 gathers of up to 32
+// bytes) in registers, about 250 registers per thread.
 #ifndef BCG_THREADS
-#define BCG_THREADS 512
-#endif
-#ifndef BCG_STAGE_BYTES
-#define BCG_STAGE_BYTES 4096
+#define BCG_THREADS 256
 #endif
 constexpr int kThreads = BCG_THREADS;    // threads per CTA of the sweep kernel
 constexpr int kWarps = kThreads / 32;    // independent tile workers per CTA
@@ -22,7 +21,6 @@ constexpr int kTileEdges = BCG_TILE_EDGES;  // max adjacency entries per tile
 constexpr int kItems = 8;                   // edges per lane in one round of a tile
 constexpr int kRoundEdges = 32 * kItems;    // a warp takes a tile's edges in rounds of this many
 static_assert(kTileEdges % kRoundEdges == 0, "a tile holds whole rounds");
-constexpr int kStageBytes = BCG_STAGE_BYTES;  // per-warp shared staging of gathered rows
 constexpr int kPushSplit = 8;            // sparse push sweeps: warps per tile
 constexpr uint16_t kUnvisited = 0xFFFFu;
 constexpr uint32_t kMaxLevel = 0xFFFDu;  // deepest level a 16-bit level can hold
@@ -50,12 +48,16 @@ __host__ __device__ constexpr int row_bytes(int S) { return ((S <= 4) ? 8 : 16) 
 
 // One unit of sweep work: vertices [v0, v1) with all their edges, or one
 // chunk [e0, e1) of the adjacency of a single high-degree vertex (hub >= 0).
+// The chunks of a hub are consecutive tiles; chunk c of a hub has its own
+// accumulator slot hslot (the hub's chunks use slots hslot - c .. hslot - c +
+// nchunks - 1), so the chunk totals can be added in chunk order.
 struct Tile {
     uint32_t v0, v1;
     uint32_t e0, e1;
-    int32_t hub;       // hub slot, -1 for an ordinary tile
+    int32_t hub;       // hub index, -1 for an ordinary tile
     uint32_t nchunks;  // chunks of this hub (1 for ordinary tiles)
-    uint32_t pad0, pad1;
+    uint32_t hslot;    // hub chunks: accumulator slot of this chunk (0 otherwise)
+    uint32_t hchunk;   // hub chunks: index c of this chunk within its hub (0 otherwise)
 };
 
 // Sweep modes.
@@ -118,14 +120,18 @@ struct BatchArgs {
     const double *mult;     // nbatch * S weight of each root's dependencies
     const uint32_t *pend;   // nbatch * S pendant sources folded into the root
     uint32_t nbatch;
-    unsigned long long *hub_acc;  // nhub * S
-    unsigned int *hub_cnt;        // nhub
+    unsigned long long *hub_acc;  // (hub chunks) * S: one slot per chunk
+    unsigned int *hub_cnt;        // nhub: chunks of the hub finished in the current sweep
     Ctrl *ctrl;
     RootStat *rstat;        // nbatch * S
     unsigned long long nnz; // adjacency entries of the pruned graph
     float push_pull_ratio;  // pull when frontier pair-edges >= ratio * unvisited pair-edges
     int directed;           // 1: adjacency is not symmetric, pull is not allowed
-    // debug outputs for a single-slot single-batch run (nullptr otherwise)
+    // debug outputs of a single-batch run (nullptr otherwise): slot k of
+    // vertex v at [k * n + v]; levels and sigma are copied after the forward
+    // pass, delta is written by the backward pass (which then runs down to
+    // level 0)
+    int32_t *dbg_level;
     unsigned long long *dbg_sigma;
     double *dbg_delta;
     // optional sweep trace (nullptr = off); trace_cnt counts records written

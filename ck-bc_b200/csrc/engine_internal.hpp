@@ -39,7 +39,7 @@ struct bcg_graph {
     uint32_t *d_anchor = nullptr, *d_reach = nullptr;
     double *d_bc = nullptr;
     Tile *d_tiles = nullptr;
-    uint32_t ntiles = 0, nhub = 0;
+    uint32_t ntiles = 0, nhub = 0, nhubchunks = 0;
     unsigned long long *d_hub_acc = nullptr;
     unsigned int *d_hub_cnt = nullptr;
     uint32_t *d_tile_of = nullptr, *d_tmark = nullptr;
@@ -74,6 +74,7 @@ struct bcg_graph {
     // closed-form tree terms wait for it
     std::vector<uint32_t> h_lab_offs, h_lab_adj;
     std::future<int> comp_job;
+    int comp_rc = BCG_OK;             // the job's result once taken from the future
     double *d_tree_acc = nullptr;     // tree vertices' closed-form bc of one run
     int sigma_mode = 0;               // 0 auto (exact, extended on overflow), 1 exact only, 2 extended
     double *d_bc_save = nullptr;      // accumulators before an automatic-mode run

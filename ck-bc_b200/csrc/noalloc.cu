@@ -13,11 +13,17 @@
 // address is kept per device for the life of the process.
 //
 // Scratch that must start at zero and is cleared by every call: the status
-// block, the sweep control block, the tile marks, the hub accumulators and
-// arrival counters, and the 16-byte tail pad of the adjacency copy (and d_bc
-// when not accumulating).  Everything else (state rows, level lists, the
-// unvisited-tile ring, roots) is written before it is read.  One scratch per
-// device: calls that overlap on the same device race on it.
+// block, the sweep control block, the tile marks, the hub arrival counters,
+// and the 16-byte tail pads of the adjacency, offsets and degree copies (and
+// d_bc when not accumulating).  Everything else (state rows, level lists, the
+// unvisited-tile ring, roots, the hub chunk slots, the saved accumulators) is
+// written before it is read.  One scratch per device: calls that overlap on the same device race
+// on it.
+//
+// Path counts: exact uint64 first; when one overflows (large grids, long
+// chains of diamonds), the accumulators saved before the sweep are put back
+// and the sweep runs again with extended-range counts (ext64.cuh), as
+// bcg_run does in its automatic mode.
 #include <algorithm>
 #include <cstdlib>
 #include <mutex>
@@ -40,6 +46,8 @@ constexpr int kNaMaxWidth = 6;
 // <= n + adj / kTileEdges
 constexpr uint64_t kNaMaxTiles = kNaMaxN + kNaMaxAdj / kTileEdges;
 constexpr uint64_t kNaMaxHubs = kNaMaxAdj / (kTileEdges + 1) + 1;  // a hub has more than kTileEdges entries
+// a hub of degree g has ceil(g / kTileEdges) <= g / kTileEdges + 1 chunks
+constexpr uint64_t kNaMaxHubChunks = kNaMaxAdj / kTileEdges + kNaMaxHubs;
 constexpr uint64_t kNaMaxSlots = kNaMaxSrc + kNaMaxWidth;
 constexpr int kNaMaxDevices = 64;
 
@@ -63,7 +71,10 @@ constexpr size_t kOffStatus = 0;
 constexpr size_t kOffCtrl = kOffStatus + up256(sizeof(NaStatus));
 constexpr size_t kOffAdj = kOffCtrl + up256(sizeof(Ctrl));
 constexpr size_t kOffVinfo = kOffAdj + up256((kNaMaxAdj + 4) * sizeof(uint32_t));
-constexpr size_t kOffTiles = kOffVinfo + up256(kNaMaxN * sizeof(uint2));
+// offsets are copied too: the sweep reads them in 16-byte aligned pieces
+// that may run 4 entries past n + 1 (zeroed tail)
+constexpr size_t kOffOffs = kOffVinfo + up256((kNaMaxN + 4) * sizeof(uint2));
+constexpr size_t kOffTiles = kOffOffs + up256((kNaMaxN + 1 + 4) * sizeof(uint32_t));
 constexpr size_t kOffTileOf = kOffTiles + up256(kNaMaxTiles * sizeof(Tile));
 constexpr size_t kOffTmark = kOffTileOf + up256(kNaMaxN * sizeof(uint32_t));
 constexpr size_t kOffLists = kOffTmark + up256(kNaMaxTiles * sizeof(uint32_t));
@@ -72,12 +83,13 @@ constexpr size_t kOffLcnt = kOffLbase + up256((kMaxLevel + 3) * sizeof(uint32_t)
 constexpr size_t kOffUlist = kOffLcnt + up256((kMaxLevel + 3) * sizeof(uint32_t));
 constexpr size_t kOffRows = kOffUlist + up256(2 * kNaMaxTiles * sizeof(uint32_t));
 constexpr size_t kOffHubAcc = kOffRows + up256(kNaMaxN * row_bytes(kNaMaxWidth));
-constexpr size_t kOffHubCnt = kOffHubAcc + up256(kNaMaxHubs * kNaMaxWidth * sizeof(unsigned long long));
+constexpr size_t kOffHubCnt = kOffHubAcc + up256(kNaMaxHubChunks * kNaMaxWidth * sizeof(unsigned long long));
 constexpr size_t kOffRoots = kOffHubCnt + up256(kNaMaxHubs * sizeof(unsigned int));
 constexpr size_t kOffPend = kOffRoots + up256(kNaMaxSlots * sizeof(uint32_t));
 constexpr size_t kOffMult = kOffPend + up256(kNaMaxSlots * sizeof(uint32_t));
 constexpr size_t kOffRstat = kOffMult + up256(kNaMaxSlots * sizeof(double));
-constexpr size_t kScratchBytes = kOffRstat + up256(kNaMaxSlots * sizeof(RootStat));
+constexpr size_t kOffBcSave = kOffRstat + up256(kNaMaxSlots * sizeof(RootStat));
+constexpr size_t kScratchBytes = kOffBcSave + up256(kNaMaxN * sizeof(double));
 static_assert(kScratchBytes <= (size_t)20 << 20, "no-allocation scratch is meant to stay under 20 MiB");
 static_assert(kOffAdj == kOffCtrl + up256(sizeof(Ctrl)) && kOffCtrl > kOffStatus,
               "status and control blocks lead the scratch so one memset clears both");
@@ -124,14 +136,15 @@ __global__ void k_na_vinfo(uint32_t n, const uint32_t *__restrict__ offs, uint2 
 }
 
 // Work tiles, the same greedy partition bcg_graph_create builds on the host:
-// runs of up to 32 consecutive vertices with at most 256 adjacency entries,
-// and vertices with more than 256 entries split into 256-entry chunks.  One
-// thread: the partition is sequential and the graphs here are small.
+// runs of up to kTileVerts (32) consecutive vertices with at most kTileEdges
+// (512 by default) adjacency entries, and vertices with more than kTileEdges
+// entries split into kTileEdges-entry chunks.  One thread: the partition is
+// sequential and the graphs here are small.
 __global__ void k_na_tiles(uint32_t n, const uint32_t *__restrict__ offs, Tile *__restrict__ tiles,
                            uint32_t *__restrict__ tile_of, NaStatus *st) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     if (st->error) return;  // offsets were rejected: nothing below may trust them
-    uint32_t nt = 0, nhub = 0, v = 0;
+    uint32_t nt = 0, nhub = 0, nchunk = 0, v = 0;
     while (v < n) {
         const uint32_t dv = offs[v + 1] - offs[v];
         if (dv > (uint32_t)kTileEdges) {
@@ -149,6 +162,8 @@ __global__ void k_na_tiles(uint32_t n, const uint32_t *__restrict__ offs, Tile *
                 t.e1 = min(offs[v + 1], t.e0 + (uint32_t)kTileEdges);
                 t.hub = (int32_t)nhub;
                 t.nchunks = nch;
+                t.hslot = nchunk++;
+                t.hchunk = c;
                 tiles[nt++] = t;
             }
             ++nhub;
@@ -313,6 +328,7 @@ extern "C" int bcg_bc_noalloc(const uint32_t *d_offsets, const uint32_t *d_adj, 
     Ctrl *d_ctrl = reinterpret_cast<Ctrl *>(scr + kOffCtrl);
     uint32_t *d_adjc = reinterpret_cast<uint32_t *>(scr + kOffAdj);
     uint2 *d_vinfo = reinterpret_cast<uint2 *>(scr + kOffVinfo);
+    uint32_t *d_offc = reinterpret_cast<uint32_t *>(scr + kOffOffs);
     Tile *d_tiles = reinterpret_cast<Tile *>(scr + kOffTiles);
     uint32_t *d_tile_of = reinterpret_cast<uint32_t *>(scr + kOffTileOf);
     uint32_t *d_tmark = reinterpret_cast<uint32_t *>(scr + kOffTmark);
@@ -325,6 +341,9 @@ extern "C" int bcg_bc_noalloc(const uint32_t *d_offsets, const uint32_t *d_adj, 
     NA_CK(cudaMemsetAsync(scr, 0, kOffAdj, st));
     if (nnz) NA_CK(cudaMemcpyAsync(d_adjc, d_adj, nnz * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
     NA_CK(cudaMemsetAsync(d_adjc + nnz, 0, 4 * sizeof(uint32_t), st));
+    NA_CK(cudaMemcpyAsync(d_offc, d_offsets, ((size_t)n + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+    NA_CK(cudaMemsetAsync(d_offc + n + 1, 0, 4 * sizeof(uint32_t), st));
+    NA_CK(cudaMemsetAsync(d_vinfo + n, 0, 4 * sizeof(uint2), st));
     k_na_check_offsets<<<(unsigned)((n + 1 + 255) / 256), 256, 0, st>>>(n, nnz, d_offsets, d_status);
     if (nnz) {
         const unsigned blocks = (unsigned)std::min<uint64_t>((nnz + 255) / 256, 148ull * 8);
@@ -341,6 +360,11 @@ extern "C" int bcg_bc_noalloc(const uint32_t *d_offsets, const uint32_t *d_adj, 
         return set_error(BCG_ERR_ARG, "invalid input: %s %llu", bad_name(hs.what), hs.index);
 
     if (!accumulate) NA_CK(cudaMemsetAsync(d_bc, 0, (size_t)n * sizeof(double), st));
+    // the caller's accumulators before the sweep: a run whose uint64 path
+    // counts overflow is redone with extended-range counts from this copy,
+    // as bcg_run does in its automatic mode
+    double *d_bc_save = reinterpret_cast<double *>(scr + kOffBcSave);
+    NA_CK(cudaMemcpyAsync(d_bc_save, d_bc, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     if (hs.nroots == 0) {
         NA_CK(cudaStreamSynchronize(st));
         return BCG_OK;
@@ -350,12 +374,11 @@ extern "C" int bcg_bc_noalloc(const uint32_t *d_offsets, const uint32_t *d_adj, 
     const uint64_t nbatch = (hs.nroots + S - 1) / S;
     const uint32_t nhub_alloc = hs.nhub ? hs.nhub : 1u;
     NA_CK(cudaMemsetAsync(d_tmark, 0, (size_t)(hs.ntiles ? hs.ntiles : 1u) * sizeof(uint32_t), st));
-    NA_CK(cudaMemsetAsync(scr + kOffHubAcc, 0, (size_t)nhub_alloc * S * sizeof(unsigned long long), st));
     NA_CK(cudaMemsetAsync(scr + kOffHubCnt, 0, (size_t)nhub_alloc * sizeof(unsigned int), st));
 
     BatchArgs a{};
     a.n = n;
-    a.offs = d_offsets;
+    a.offs = d_offc;
     a.adj = d_adjc;
     a.vinfo = d_vinfo;
     a.tiles = d_tiles;
@@ -381,16 +404,31 @@ extern "C" int bcg_bc_noalloc(const uint32_t *d_offsets, const uint32_t *d_adj, 
     a.push_pull_ratio = 0.2f;
     if (const char *e = getenv("BCG_PUSH_PULL_RATIO")) a.push_pull_ratio = (float)atof(e);
     a.directed = 0;
-    int grid = 0;
-    rc = launch_sweep((int)S, a, st, &grid);
-    if (rc) return rc;
-    int flags[2] = {0, 0};  // Ctrl::error, Ctrl::overflow
-    NA_CK(cudaMemcpyAsync(flags, &d_ctrl->error, sizeof(flags), cudaMemcpyDeviceToHost, st));
-    NA_CK(cudaStreamSynchronize(st));
-    if (flags[1] || flags[0] == BCG_ERR_OVERFLOW)
-        return set_error(BCG_ERR_OVERFLOW, "a shortest-path count exceeded 2^64");
-    if (flags[0])
-        return set_error(flags[0], "device reported error %d (%s)", flags[0],
-                         flags[0] == BCG_ERR_TIMEOUT ? "a bounded wait gave up" : "level limit exceeded");
+    for (int pass = 0; pass < 2; ++pass) {
+        const bool ext = pass == 1;
+        if (ext) {
+            // overflow: restore the accumulators and clear the scratch the
+            // aborted sweep left behind (control block, tile marks, hub
+            // arrival counters), then run extended counts
+            NA_CK(cudaMemcpyAsync(d_bc, d_bc_save, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            NA_CK(cudaMemsetAsync(d_ctrl, 0, sizeof(Ctrl), st));
+            NA_CK(cudaMemsetAsync(d_tmark, 0, (size_t)(hs.ntiles ? hs.ntiles : 1u) * sizeof(uint32_t), st));
+            NA_CK(cudaMemsetAsync(scr + kOffHubCnt, 0, (size_t)nhub_alloc * sizeof(unsigned int), st));
+        }
+        int grid = 0;
+        rc = launch_sweep((int)S, a, st, &grid, ext);
+        if (rc) return rc;
+        int flags[2] = {0, 0};  // Ctrl::error, Ctrl::overflow
+        NA_CK(cudaMemcpyAsync(flags, &d_ctrl->error, sizeof(flags), cudaMemcpyDeviceToHost, st));
+        NA_CK(cudaStreamSynchronize(st));
+        if (flags[1] || flags[0] == BCG_ERR_OVERFLOW) {
+            if (!ext) continue;
+            return set_error(BCG_ERR_OVERFLOW, "a shortest-path count exceeded the extended range");
+        }
+        if (flags[0])
+            return set_error(flags[0], "device reported error %d (%s)", flags[0],
+                             flags[0] == BCG_ERR_TIMEOUT ? "a bounded wait gave up" : "level limit exceeded");
+        return BCG_OK;
+    }
     return BCG_OK;
 }

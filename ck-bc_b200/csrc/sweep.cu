@@ -25,25 +25,39 @@
 // a 32-byte row for S = 3, so one gathered sector answers both "is this
 // neighbour at the wanted level" and "what is its value" for all slots.  With
 // S = 3 the rows of a 1.5M-vertex graph take 47 MB and stay in the 126 MB L2
-// while the adjacency streams past with an evict-first policy.
+// while the adjacency streams past with an evict-first policy.  A neighbour's
+// row is gathered with one 32-byte load per lane (two for S = 6): a scattered
+// load costs the L1 one pass per distinct line it touches, so one 32-byte
+// access per row halves those passes against two 16-byte ones.
 //
 // Work decomposition.  Vertices are cut into static tiles of <= 32
 // consecutive vertices and <= kTileEdges (512) adjacency entries; a vertex
-// with more entries is split into kTileEdges-entry chunks whose partial sums
-// meet in hub_acc (the last chunk to arrive finishes the vertex).  One warp
-// works on one tile at a time with no CTA-wide synchronisation: lane j owns
-// vertex j, the tile's active edges are taken in rounds of <= 256, and each
-// round is cut into contiguous runs of <= 8 per lane (merge-path over the
-// warp's exclusive scan of active degrees).  A tile's fixed costs (its two
-// list and descriptor reads, row loads, scan and finishing writes) are about
-// two thirds of a dense sweep at 256 entries per tile, hence the larger tiles.  Each lane loads its
-// run's adjacency entries, then issues cp.async copies of all their rows into
-// its slice of the warp's shared staging buffer, so a tile costs two dependent
-// global round trips however many edges are in flight.  Push and backward
-// sweeps walk only the tiles on the level's list (tiles holding a vertex first
+// with more entries is split into kTileEdges-entry chunks ("hub" chunks).
+// One warp works on one tile at a time with no CTA-wide synchronisation: lane
+// j owns vertex j, the tile's active edges are taken in rounds of <= 256, and
+// each round is cut into contiguous runs of <= 8 per lane (merge-path over the
+// warp's exclusive scan of active degrees).  Each warp pipelines its tiles:
+// while it works on one tile, the next tile's adjacency range is already
+// being copied into the other half of its shared buffer by one bulk
+// asynchronous copy (cp.async.bulk, completion on an mbarrier), and the next
+// tile's own rows, degree/reach words and row starts are in flight to
+// registers.  A tile then costs one dependent round trip per round (the row
+// gathers) instead of one more for its own data.  Push and backward sweeps
+// walk only the tiles on the level's list (tiles holding a vertex first
 // reached at that level, for any slot; a sparse push splits each tile over
 // kPushSplit warps); pull sweeps walk the tiles that still hold an unvisited
 // vertex (all tiles in the first pull of a batch).
+//
+// Deterministic sums.  A vertex's sum over its neighbours (sigma of parents
+// in a pull, X of children in the backward pass) is formed in a fixed order:
+// each lane adds its run's terms in adjacency order; the partial sums of a
+// vertex whose edges span several lanes are combined by a segmented warp scan
+// in lane order; the per-round totals are added into the vertex's shared
+// accumulator by the single lane that ends the vertex in that round, rounds
+// in order; a hub's chunk totals are stored in one slot per chunk and added in
+// chunk order by the chunk that arrives last.  No floating-point atomics are
+// used, so a run's results are bitwise reproducible and a source's
+// contribution does not depend on the batch it shares.
 #include <cstdio>
 
 #include "bcg.h"
@@ -74,23 +88,70 @@ __device__ __forceinline__ unsigned long long evict_first_policy() {
     return pol;
 }
 
-// Asynchronous global -> shared copies (completion: cp_wait_all).
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+__device__ __forceinline__ unsigned long long evict_normal_policy() {
+    unsigned long long pol;
+    asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
 }
-__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+
+__device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+// ---- mbarrier + bulk copy (one 1-D async copy per tile adjacency range)
+__device__ __forceinline__ void mbar_init(unsigned long long *bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
 }
-// 16-byte copy of streamed data (L2 only, evict-first policy).
-__device__ __forceinline__ void cp_async16_stream(void *smem, const void *gmem, unsigned long long pol) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(s), "l"(gmem), "l"(pol)
-                 : "memory");
+__device__ __forceinline__ void mbar_init_fence() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
-__device__ __forceinline__ void cp_wait_all() {
-    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+// Copies [src, src + bytes) to dst (both 16-byte aligned, bytes a nonzero
+// multiple of 16), completing `bytes` of transfer on the barrier at shared
+// address bar.
+__device__ __forceinline__ void bulk_copy(void *dst, const void *src, uint32_t bytes, unsigned bar,
+                                          unsigned long long pol) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(bar), "l"(pol)
+        : "memory");
+}
+// Bounded wait for phase `parity` of the barrier; false when wait_ns ran out.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, uint32_t parity, unsigned long long wait_ns) {
+    const unsigned b = smem_addr(bar);
+    unsigned long long t0 = 0;
+    for (uint32_t spins = 0;; ++spins) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(b), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (spins == 0) t0 = global_ns();
+        else if ((spins & 15u) == 0 && global_ns() - t0 > wait_ns) return false;
+    }
+}
+
+// ---- loads of state rows into registers (rows are 16, 32 or 64 bytes, aligned)
+template <int NW>
+__device__ __forceinline__ void ld_row(const unsigned char *row, uint32_t (&w)[NW]) {
+    if (NW == 4) {
+        asm volatile("ld.global.v4.u32 {%0,%1,%2,%3}, [%4];" : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]) : "l"(row));
+    } else {
+#pragma unroll
+        for (int h = 0; h < NW / 8; ++h)
+            asm volatile("ld.global.v8.u32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                         : "=r"(w[8 * h]), "=r"(w[8 * h + 1]), "=r"(w[8 * h + 2]), "=r"(w[8 * h + 3]), "=r"(w[8 * h + 4]),
+                           "=r"(w[8 * h + 5]), "=r"(w[8 * h + 6]), "=r"(w[8 * h + 7])
+                         : "l"(row + 32 * h));
+    }
+}
+// The level block (first 8 or 16 bytes) of a row.
+template <int NL>
+__device__ __forceinline__ void ld_lvl(const unsigned char *row, uint32_t (&w)[NL]) {
+    if (NL == 2)
+        asm volatile("ld.global.v2.u32 {%0,%1}, [%2];" : "=r"(w[0]), "=r"(w[1]) : "l"(row));
+    else
+        asm volatile("ld.global.v4.u32 {%0,%1,%2,%3}, [%4];" : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]) : "l"(row));
 }
 
 // Software grid barrier (all CTAs co-resident: cooperative launch).  One
@@ -99,7 +160,8 @@ __device__ __forceinline__ void cp_wait_all() {
 // reset between barriers.  Thread 0 also reads the error and overflow flags
 // once, after every CTA has arrived, and hands the verdict to its CTA through
 // shared memory.  Returns false when any CTA recorded an error or an overflow,
-// in which case the caller returns.
+// in which case the caller returns.  The fences around the wait make every
+// write before the barrier (any CTA) visible to every read after it.
 __device__ bool grid_sync(Ctrl *c, unsigned int nblocks, unsigned long long wait_ns) {
     __shared__ int ok;
     __syncthreads();
@@ -150,37 +212,31 @@ template <int S>
 __device__ __forceinline__ unsigned long long *val_at(unsigned char *row, int k) {
     return reinterpret_cast<unsigned long long *>(row + RowGeom<S>::kLvlBytes) + k;
 }
-// Whole-row global load into words.
-template <int S>
-__device__ __forceinline__ void load_row_words(const unsigned char *row, uint32_t (&w)[RowGeom<S>::kWords]) {
-    const uint4 *p = reinterpret_cast<const uint4 *>(row);
-#pragma unroll
-    for (int h = 0; h < RowGeom<S>::kVec; ++h) {
-        const uint4 t = p[h];
-        w[4 * h] = t.x; w[4 * h + 1] = t.y; w[4 * h + 2] = t.z; w[4 * h + 3] = t.w;
-    }
-}
+
+// Adjacency entries a tile buffer holds: the range [e0, e1) widened to
+// 16-byte boundaries on both sides (<= 3 entries each).
+constexpr int kAdjBuf = kTileEdges + 8;
+static_assert((kAdjBuf * 4) % 16 == 0, "tile buffers keep 16-byte alignment");
 
 // Per-warp scratch.
 template <int S>
 struct WarpSmem {
-    uint32_t pre[kTileVerts + 1];
-    uint32_t eb[kTileVerts];
-    uint32_t mask[kTileVerts];
+    alignas(128) uint32_t adjs[2][kAdjBuf];  // tile adjacency, double-buffered (bulk-copy targets)
+    alignas(16) uint4 rows[2][kTileVerts * RowGeom<S>::kVec];  // the tile's own state rows (bulk-copy targets)
+    alignas(16) uint2 vbuf[2][kTileVerts + 2];   // their {degree, reach} words, from an even vertex on
+    alignas(16) uint32_t obuf[2][kTileVerts + 8];  // their row starts, from a multiple-of-4 vertex on
+    unsigned long long mbar[2];              // completion of the four copies of buffer b
+    uint32_t pre[kTileVerts + 1];            // exclusive scan of active degrees
+    uint32_t eb[kTileVerts];                 // start of vertex j's active edges in its adjs buffer
+    uint32_t mask[kTileVerts];               // active slots of vertex j
     uint32_t app[2 * 32];   // buffered appends to the next level's list
     uint32_t uapp[2 * 32];  // buffered appends to the unvisited-tile ring
     uint32_t napp, nuapp;
-    unsigned long long acc[kTileVerts][S];
-    unsigned long long own[kTileVerts][S];
-    uint4 stage[kStageBytes / 16];  // rows gathered by cp.async, lane-sliced
-    // the tile's adjacency entries (aligned-down start, <= kTileEdges + 3 entries)
-    alignas(16) uint32_t adjs[kTileEdges + 16];
+    unsigned long long acc[kTileVerts][S];   // per-vertex sums of the tile (one writer per round)
+    unsigned long long own[kTileVerts][S];   // push: sigma of the frontier vertex's active slots
     // per-warp discovery totals of the sweep (LaneCounts layout)
     unsigned long long cnt[2 + 3 * S];
 };
-
-// push sweeps stage one 16-byte level block per edge of the lane's run
-static_assert(kStageBytes >= kItems * 32 * 16, "stage must hold a push tile's level blocks");
 
 template <int S>
 struct Smem {
@@ -196,6 +252,26 @@ struct Smem {
 
 template <int S>
 size_t smem_bytes() { return sizeof(Smem<S>); }
+
+// A tile descriptor held one 32-bit word per lane (lanes 0..7), so a warp's
+// pipeline of drawn tiles costs one register per tile; unpacked by shuffles
+// when the tile comes up.
+__device__ __forceinline__ uint32_t tile_word(const Tile *tiles, uint32_t ti) {
+    const unsigned lane = threadIdx.x & 31;
+    return lane < 8 ? reinterpret_cast<const uint32_t *>(tiles + ti)[lane] : 0u;
+}
+__device__ __forceinline__ Tile tile_unpack(uint32_t tw) {
+    Tile T;
+    T.v0 = __shfl_sync(0xffffffffu, tw, 0);
+    T.v1 = __shfl_sync(0xffffffffu, tw, 1);
+    T.e0 = __shfl_sync(0xffffffffu, tw, 2);
+    T.e1 = __shfl_sync(0xffffffffu, tw, 3);
+    T.hub = (int32_t)__shfl_sync(0xffffffffu, tw, 4);
+    T.nchunks = __shfl_sync(0xffffffffu, tw, 5);
+    T.hslot = __shfl_sync(0xffffffffu, tw, 6);
+    T.hchunk = __shfl_sync(0xffffffffu, tw, 7);
+    return T;
+}
 
 // Parameters of one sweep, identical in every warp.
 struct SweepCtx {
@@ -379,7 +455,7 @@ __device__ __forceinline__ void flag_overflow(Ctrl *c) { c->overflow = 1; }
 // Value arithmetic of a sweep.  Forward sweeps sum sigma values, backward
 // sweeps sum X = (1 + delta) / sigma values; with EXT both are extended-range
 // numbers (ext64.cuh), otherwise sigma is an exact uint64 (a wrapped sum sets
-// the overflow flag) and X a double.
+// the overflow flag) and X a double.  vsum(x, y) adds y after x.
 template <bool EXT, int MODE>
 __device__ __forceinline__ unsigned long long vsum(unsigned long long x, unsigned long long y, const BatchArgs &a) {
     if (EXT) return ext_add(x, y);
@@ -391,72 +467,67 @@ __device__ __forceinline__ unsigned long long vsum(unsigned long long x, unsigne
     return t;
 }
 
-// *p += y atomically (p in global or shared memory).  The extended form is a
-// compare-and-swap retry loop: each failed attempt means another thread's add
-// went through, so the loop always ends.
-template <bool EXT, int MODE>
-__device__ __forceinline__ void vatomic(unsigned long long *p, unsigned long long y, const BatchArgs &a) {
+// *p += y atomically in global memory (push sweeps: integer sigma, or the
+// extended form as a compare-and-swap retry loop; each failed attempt means
+// another thread's add went through, so the loop always ends).  Integer and
+// extended sums of exact counts do not depend on the order of the adds.
+template <bool EXT>
+__device__ __forceinline__ void sigma_atomic(unsigned long long *p, unsigned long long y, const BatchArgs &a) {
     if (EXT) {
         unsigned long long old = *reinterpret_cast<volatile unsigned long long *>(p), seen;
         do {
             seen = old;
             old = atomicCAS(p, seen, ext_add(seen, y));
         } while (old != seen);
-    } else if (MODE == kBwd) {
-        atomicAdd(reinterpret_cast<double *>(p), __longlong_as_double((long long)y));
     } else {
         const unsigned long long old = atomicAdd(p, y);
         if (old + y < y) flag_overflow(a.ctrl);
     }
 }
 
-template <int S, int MODE, bool EXT>
-__device__ __forceinline__ void flush_run(const BatchArgs &a, WarpSmem<S> &ws, uint32_t j,
-                                          unsigned long long (&run)[S]) {
-#pragma unroll
-    for (int k = 0; k < S; ++k) {
-        if (!run[k]) continue;
-        vatomic<EXT, MODE>(&ws.acc[j][k], run[k], a);
-        run[k] = 0ull;
-    }
+__device__ __forceinline__ unsigned long long shfl_up64(unsigned long long v, int o) {
+    return __shfl_up_sync(0xffffffffu, v, o);
 }
 
-// One tile (or one part of a split tile), processed by one warp.
+// One tile (or one part of a split tile), processed by one warp.  The tile's
+// adjacency (copied from entry T.e0 & ~3 on), own rows, degree/reach words
+// and row starts are in buffer `buf` of the warp's scratch (tile_fetch).
 template <int S, int MODE, bool EXT>
 __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint32_t ti, const Tile &T,
-                          uint32_t part, const SweepCtx &x) {
-    constexpr int R = RowGeom<S>::kBytes;
+                          uint32_t part, const SweepCtx &x, int buf) {
     constexpr int NW = RowGeom<S>::kWords;
+    constexpr int NV = RowGeom<S>::kVec;
     const unsigned lane = threadIdx.x & 31;
     const uint32_t d = x.d;
     const uint16_t dl = (uint16_t)d;
     const bool hub = T.hub >= 0;
     const uint32_t nv = T.v1 - T.v0;
-    uint32_t deg_act = 0, m = 0;
-    uint2 vi = make_uint2(0, 0);
-    const unsigned long long pol = evict_first_policy();
-    // ---- phase 1 (one round trip): the tile's adjacency range [e0, e1) is
-    // copied to shared memory in 16-byte chunks from the aligned-down start,
-    // while each lane loads its vertex's row, degree/reach and row start
+    const uint32_t *adjs = ws.adjs[buf];
     const uint32_t ab = T.e0 & ~3u;
-    {
-        const uint32_t nch16 = (T.e1 - ab + 3) >> 2;  // <= kTileEdges / 4 + 1
-        for (uint32_t c = lane; c < nch16; c += 32) cp_async16_stream(ws.adjs + 4 * c, a.adj + ab + 4 * c, pol);
-    }
-    uint32_t w[NW];
+    uint32_t deg_act = 0, m = 0;
+    // the lane's own row, as copied with the tile (levels, and sigma of the
+    // slots whose level is d); read again from the buffer where needed
+    auto own_row = [&](uint32_t (&ow)[NW]) {
+#pragma unroll
+        for (int h = 0; h < NV; ++h) {
+            const uint4 t = ws.rows[buf][lane * NV + h];
+            ow[4 * h] = t.x; ow[4 * h + 1] = t.y; ow[4 * h + 2] = t.z; ow[4 * h + 3] = t.w;
+        }
+    };
+    // the lane's degree/reach word and row start, as copied with the tile
+    uint2 vi = make_uint2(0u, 0u);
     uint32_t ob = 0;
     if (lane < nv) {
-        const uint32_t v = T.v0 + lane;
-        load_row_words<S>(row_of<S>(a, v), w);
-        vi = a.vinfo[v];
-        ob = a.offs[v];
+        vi = ws.vbuf[buf][(T.v0 & 1u) + lane];
+        ob = ws.obuf[buf][(T.v0 & 3u) + lane];
     }
-    cp_wait_all();
-    __syncwarp();
+    // ---- phase 1: the lane's vertex (its data arrived with the tile)
     if (lane < nv) {
+        uint32_t ow[NW];
+        own_row(ow);
 #pragma unroll
         for (int k = 0; k < S; ++k) {
-            const uint16_t L = w_lvl(w, k);
+            const uint16_t L = w_lvl(ow, k);
             if (MODE == kFwdPull) m |= (uint32_t)(L == kUnvisited) << k;
             else m |= (uint32_t)(L == dl) << k;
         }
@@ -468,14 +539,13 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
             if (ee < eb) ee = eb;
             deg_act = ee - eb;
             if (MODE == kBwd && d == x.D) deg_act = 0;
-            ws.eb[lane] = eb;
+            ws.eb[lane] = eb - ab;
             if (MODE != kFwdPush) {
 #pragma unroll
                 for (int k = 0; k < S; ++k) ws.acc[lane][k] = 0ull;
-            }
-            if (MODE != kFwdPull) {
+            } else {
 #pragma unroll
-                for (int k = 0; k < S; ++k) ws.own[lane][k] = ((m >> k) & 1u) ? w_val<S>(w, k) : 0ull;
+                for (int k = 0; k < S; ++k) ws.own[lane][k] = ((m >> k) & 1u) ? w_val<S>(ow, k) : 0ull;
             }
         }
         ws.mask[lane] = m;
@@ -504,11 +574,12 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
         const uint32_t per = (r1 - r0 + 31) / 32;  // <= kItems
         const uint32_t i0 = r0 + lane * per;
         const uint32_t i1 = min(r1, i0 + per);
+        const bool has = i0 < i1;
         // the run's vertex j, the end of its edges (nxt) and the offset of its
         // edges in adjs (base + i) stay in registers; they are reloaded from
         // shared memory only when the run crosses into the next vertex
         uint32_t j = 0, nxt = 0, base = 0;
-        if (i0 < i1) {
+        if (has) {
             uint32_t lo = 0, hi = nv;
             while (hi - lo > 1) {
                 const uint32_t mid = (lo + hi) >> 1;
@@ -516,50 +587,58 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
             }
             j = lo;
             nxt = ws.pre[j + 1];
-            base = ws.eb[j] - ab - ws.pre[j];
+            base = ws.eb[j] - ws.pre[j];
         }
-        uint32_t jj[kItems], uu[kItems];
+        const uint32_t jfirst = j, nfirst = nxt;
+        uint32_t uu[kItems];
 #pragma unroll
         for (int q = 0; q < kItems; ++q) {
             const uint32_t i = i0 + q;
+            uu[q] = 0;
             if (i < i1) {
                 if (i >= nxt) {
                     do {
                         ++j;
                         nxt = ws.pre[j + 1];
                     } while (i >= nxt);
-                    base = ws.eb[j] - ab - ws.pre[j];
+                    base = ws.eb[j] - ws.pre[j];
                 }
-                jj[q] = j;
-                uu[q] = ws.adjs[base + i];
+                uu[q] = adjs[base + i];
             }
         }
-        if (MODE == kFwdPush) {
-            // stage the targets' level blocks (slot q of lane l at stage[q*32 + l],
-            // bank-conflict free), then claim / add with atomics
-            constexpr int LB = RowGeom<S>::kLvlBytes;
-            LaneCounts<S> cnt;
-#pragma unroll
-            for (int q = 0; q < kItems; ++q) {
-                if (i0 + q >= i1) continue;
-                if (LB == 8) cp_async8(ws.stage + q * 32 + lane, row_of<S>(a, uu[q]));
-                else cp_async16(ws.stage + q * 32 + lane, row_of<S>(a, uu[q]));
+        // the walk again while the loads are in flight: vertex of item i
+        j = jfirst;
+        nxt = nfirst;
+        auto vertex_of = [&](uint32_t i) -> uint32_t {
+            if (i >= nxt) {
+                do {
+                    ++j;
+                    nxt = ws.pre[j + 1];
+                } while (i >= nxt);
             }
-            cp_wait_all();
+            return j;
+        };
+        if (MODE == kFwdPush) {
+            // the targets' level blocks, then claim / add with atomics
+            constexpr int NL = RowGeom<S>::kLvlBytes / 4;
+            LaneCounts<S> cnt;
+            uint32_t lw[kItems][NL];
+#pragma unroll
+            for (int q = 0; q < kItems; ++q)
+                if (i0 + q < i1) ld_lvl<NL>(row_of<S>(a, uu[q]), lw[q]);
 #pragma unroll
             for (int q = 0; q < kItems; ++q) {
                 uint32_t app = kNoTile;
                 if (i0 + q < i1) {
-                    const uint32_t jm = ws.mask[jj[q]];
+                    const uint32_t jq = vertex_of(i0 + q);
+                    const uint32_t jm = ws.mask[jq];
                     const uint32_t wv = uu[q];
-                    const uint4 lw4 = ws.stage[q * 32 + lane];
-                    const uint32_t lwords[4] = {lw4.x, lw4.y, lw4.z, lw4.w};
                     unsigned char *wrow = row_of<S>(a, wv);
                     bool claimed_any = false;
 #pragma unroll
                     for (int k = 0; k < S; ++k) {
                         if (!((jm >> k) & 1u)) continue;
-                        const uint16_t L = w_lvl(lwords, k);
+                        const uint16_t L = w_lvl(lw[q], k);
                         bool take = (L == (uint16_t)(d + 1));
                         if (L == kUnvisited) {
                             const uint16_t old = atomicCAS(reinterpret_cast<unsigned short *>(lvl_at(wrow, k)),
@@ -572,9 +651,7 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
                                 take = (old == (uint16_t)(d + 1));
                             }
                         }
-                        if (take) {
-                            vatomic<EXT, kFwdPull>(val_at<S>(wrow, k), ws.own[jj[q]][k], a);
-                        }
+                        if (take) sigma_atomic<EXT>(val_at<S>(wrow, k), ws.own[jq][k], a);
                     }
                     if (claimed_any) app = claim_tile(a, wv, x.key_next);
                 }
@@ -582,66 +659,100 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
             }
             flush_counts<S>(ws, cnt);
         } else {
-            // stage the neighbours' whole rows, then sum the matching values
-            constexpr int E = (kStageBytes / (32 * R)) < kItems ? (kStageBytes / (32 * R)) : kItems;
-            static_assert(kItems % E == 0, "staging rounds must divide the run");
+            // gather the neighbours' rows (kHalf at a time: all 8 for rows of
+            // up to 32 bytes, 4 for 64-byte rows) and sum the matching values
+            // of each vertex in adjacency order
+            constexpr int kHalf = (NW <= 8) ? kItems : kItems / 2;
             const uint16_t want = (MODE == kFwdPull) ? dl : (uint16_t)(d + 1);
-            // 16-byte chunk h of lane l's row q sits at stage[(q*H + h)*32 + l]:
-            // a warp's accesses hit 32 consecutive 16-byte slots (no bank conflicts)
-            constexpr int H = R / 16;
-            unsigned long long run[S];
+            unsigned long long run[S], head[S];
 #pragma unroll
-            for (int k = 0; k < S; ++k) run[k] = 0ull;
-            uint32_t runj = (i0 < i1) ? jj[0] : 0u;
-            uint32_t runm = ws.mask[runj];
+            for (int k = 0; k < S; ++k) { run[k] = 0ull; head[k] = 0ull; }
+            uint32_t runj = jfirst;
+            uint32_t runm = has ? ws.mask[runj] : 0u;
+            bool split_run = false;  // the run has left its first vertex (head[] holds its part)
 #pragma unroll
-            for (int r = 0; r < kItems / E; ++r) {
+            for (int h0 = 0; h0 < kItems; h0 += kHalf) {
+                uint32_t wr[kHalf][NW];
 #pragma unroll
-                for (int q = 0; q < E; ++q) {
-                    const int idx = r * E + q;
-                    if (i0 + idx < i1) {
-                        const uint4 *src = reinterpret_cast<const uint4 *>(row_of<S>(a, uu[idx]));
+                for (int q = 0; q < kHalf; ++q)
+                    if (i0 + h0 + q < i1) ld_row<NW>(row_of<S>(a, uu[h0 + q]), wr[q]);
 #pragma unroll
-                        for (int h = 0; h < H; ++h) cp_async16(ws.stage + (q * H + h) * 32 + lane, src + h);
-                    }
-                }
-                cp_wait_all();
-#pragma unroll
-                for (int q = 0; q < E; ++q) {
-                    const int idx = r * E + q;
+                for (int q = 0; q < kHalf; ++q) {
+                    const int idx = h0 + q;
                     if (i0 + idx >= i1) continue;
-                    if (jj[idx] != runj) {
-                        flush_run<S, MODE, EXT>(a, ws, runj, run);
-                        runj = jj[idx];
-                        runm = ws.mask[runj];
-                    }
-                    const uint32_t jm = runm;
-                    uint32_t wr[RowGeom<S>::kWords];
+                    const uint32_t jq = vertex_of(i0 + idx);
+                    if (jq != runj) {
+                        if (!split_run) {
 #pragma unroll
-                    for (int h = 0; h < H; ++h) {
-                        const uint4 t = ws.stage[(q * H + h) * 32 + lane];
-                        wr[4 * h] = t.x; wr[4 * h + 1] = t.y; wr[4 * h + 2] = t.z; wr[4 * h + 3] = t.w;
+                            for (int k = 0; k < S; ++k) head[k] = run[k];
+                            split_run = true;
+                        } else {
+                            // a vertex wholly inside this lane's run: its round total
+#pragma unroll
+                            for (int k = 0; k < S; ++k) ws.acc[runj][k] = vsum<EXT, MODE>(ws.acc[runj][k], run[k], a);
+                        }
+#pragma unroll
+                        for (int k = 0; k < S; ++k) run[k] = 0ull;
+                        runj = jq;
+                        runm = ws.mask[runj];
                     }
 #pragma unroll
                     for (int k = 0; k < S; ++k) {
-                        if (!((jm >> k) & 1u) || w_lvl(wr, k) != want) continue;
-                        run[k] = vsum<EXT, MODE>(run[k], w_val<S>(wr, k), a);
+                        if (!((runm >> k) & 1u) || w_lvl(wr[q], k) != want) continue;
+                        run[k] = vsum<EXT, MODE>(run[k], w_val<S>(wr[q], k), a);
                     }
                 }
             }
-            if (i0 < i1) flush_run<S, MODE, EXT>(a, ws, runj, run);
+            // Partial sums of vertices that span lanes, combined in lane
+            // order: a segmented inclusive scan of the run tails keyed by
+            // their vertex (keys do not decrease with the lane).
+            const uint32_t key_last = has ? runj : 0xFFFFFFFFu;
+            const uint32_t key_first = has ? jfirst : 0xFFFFFFFEu;
+            unsigned long long sc[S];
+#pragma unroll
+            for (int k = 0; k < S; ++k) sc[k] = run[k];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t ko = __shfl_up_sync(0xffffffffu, key_last, o);
+                const bool same = lane >= (unsigned)o && ko == key_last;
+#pragma unroll
+                for (int k = 0; k < S; ++k) {
+                    const unsigned long long y = shfl_up64(sc[k], o);
+                    if (same) sc[k] = vsum<EXT, MODE>(y, sc[k], a);
+                }
+            }
+            const uint32_t kprev = __shfl_up_sync(0xffffffffu, key_last, 1);
+            const uint32_t knext = __shfl_down_sync(0xffffffffu, key_first, 1);
+            const bool carry_in = lane > 0 && kprev == key_first;
+            unsigned long long carry[S];
+#pragma unroll
+            for (int k = 0; k < S; ++k) carry[k] = shfl_up64(sc[k], 1);
+            if (has) {
+                if (split_run) {
+                    // the run's first vertex ends in this lane: earlier lanes' part, then this one's
+#pragma unroll
+                    for (int k = 0; k < S; ++k) {
+                        const unsigned long long t = carry_in ? vsum<EXT, MODE>(carry[k], head[k], a) : head[k];
+                        ws.acc[jfirst][k] = vsum<EXT, MODE>(ws.acc[jfirst][k], t, a);
+                    }
+                }
+                if (lane == 31 || knext != key_last) {
+                    // the last lane holding the run's last vertex adds the vertex's round total
+#pragma unroll
+                    for (int k = 0; k < S; ++k) ws.acc[key_last][k] = vsum<EXT, MODE>(ws.acc[key_last][k], sc[k], a);
+                }
+            }
+            __syncwarp();
         }
     }
     __syncwarp();
     if (MODE == kFwdPush) return;
 
-    // ---- hub chunks meet in hub_acc; the last chunk to arrive finishes the vertex
+    // ---- hub chunks: each chunk stores its total in its own slot; the chunk
+    // that arrives last adds the slots in chunk order and finishes the vertex
     if (hub) {
-        const uint32_t hm = ws.mask[0];
-        unsigned long long *hacc = a.hub_acc + (size_t)T.hub * S;
-        if (lane < (unsigned)S && ((hm >> lane) & 1u)) {
-            vatomic<EXT, MODE>(hacc + lane, ws.acc[0][lane], a);
-        }
+        unsigned long long *slot0 = a.hub_acc + (size_t)(T.hslot - T.hchunk) * S;
+        if (lane < (unsigned)S) __stcg(slot0 + (size_t)T.hchunk * S + lane, ws.acc[0][lane]);
         __threadfence();
         __syncwarp();
         uint32_t last = 0;
@@ -649,7 +760,11 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
         last = __shfl_sync(0xffffffffu, last, 0);
         if (!last) return;
         __threadfence();
-        if (lane < (unsigned)S) ws.acc[0][lane] = atomicExch(hacc + lane, 0ull);
+        if (lane < (unsigned)S) {
+            unsigned long long s = __ldcg(slot0 + lane);
+            for (uint32_t c = 1; c < T.nchunks; ++c) s = vsum<EXT, MODE>(s, __ldcg(slot0 + (size_t)c * S + lane), a);
+            ws.acc[0][lane] = s;
+        }
         if (lane == 0) atomicExch(a.hub_cnt + T.hub, 0u);
         __syncwarp();
     }
@@ -677,25 +792,27 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
         } else {
             double add = 0.0;
             const double reach = (double)vi.y;
+            uint32_t ow[NW];
+            own_row(ow);
 #pragma unroll
             for (int k = 0; k < S; ++k) {
                 if (!((m >> k) & 1u)) continue;
                 double delta;
+                const unsigned long long sgv = w_val<S>(ow, k);
                 if (EXT) {
                     // sigma * sum X is a dependency count (in double range)
                     // even where sigma and X are not
-                    const unsigned long long sig = ws.own[lane][k];
-                    delta = reach + ext_to_double(ext_mul(sig, ws.acc[lane][k]));
-                    *val_at<S>(vrow, k) = ext_div(1.0 + delta, sig);
+                    delta = reach + ext_to_double(ext_mul(sgv, ws.acc[lane][k]));
+                    *val_at<S>(vrow, k) = ext_div(1.0 + delta, sgv);
                 } else {
-                    const double sig = (double)ws.own[lane][k];
+                    const double sig = (double)sgv;
                     const double acc = __longlong_as_double((long long)ws.acc[lane][k]);
                     delta = reach + sig * acc;
                     const double xo = (1.0 + delta) / sig;
                     *val_at<S>(vrow, k) = (unsigned long long)__double_as_longlong(xo);
                 }
                 if (d > 0) add += sm.mult[k] * delta;
-                if (a.dbg_delta) a.dbg_delta[v] = delta;
+                if (a.dbg_delta) a.dbg_delta[(size_t)k * a.n + v] = delta;
             }
             if (d > 0) a.bc[a.ext ? a.ext[v] : v] += add;
         }
@@ -712,6 +829,46 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
     }
 }
 
+// Starts the copy of tile T's data into buffer `buf` of the warp and its
+// lanes' registers: the adjacency range (one bulk copy by lane 0) and, per
+// lane, the row, degree/reach word and row start of vertex T.v0 + lane.
+// Four 1-D bulk copies, issued by lane 0 and completing on the buffer's
+// mbarrier: the adjacency range [e0, e1) from e0 & ~3 on (up to 3 entries
+// either side: the adjacency has a 4-entry tail pad), the rows of [v0, v1),
+// their {degree, reach} words from v0 & ~1 on and their row starts from
+// v0 & ~3 on (vinfo and offs have 4 entries of tail padding).  Every source
+// and destination is 16-byte aligned and every size a multiple of 16.
+template <int S>
+__device__ __forceinline__ void tile_fetch(const BatchArgs &a, WarpSmem<S> &ws, int buf, uint32_t tw,
+                                           unsigned long long pol) {
+    const unsigned lane = threadIdx.x & 31;
+    const uint32_t v0 = __shfl_sync(0xffffffffu, tw, 0), v1 = __shfl_sync(0xffffffffu, tw, 1);
+    const uint32_t e0 = __shfl_sync(0xffffffffu, tw, 2), e1 = __shfl_sync(0xffffffffu, tw, 3);
+    __syncwarp();  // every lane is done with the buffer's previous tile
+    if (lane == 0) {
+        const uint32_t ab = e0 & ~3u, ae = (e1 + 3u) & ~3u;
+        const uint32_t vb = v0 & ~1u, ve = (v1 + 1u) & ~1u;
+        const uint32_t obb = v0 & ~3u, obe = (v1 + 3u) & ~3u;
+        const uint32_t abytes = (ae - ab) * 4u;
+        const uint32_t rbytes = (v1 - v0) * (uint32_t)RowGeom<S>::kBytes;
+        const uint32_t vbytes = (ve - vb) * 8u;
+        const uint32_t obytes = (obe - obb) * 4u;
+        const unsigned b = smem_addr(&ws.mbar[buf]);
+        // rows were written by other CTAs' generic stores before the last
+        // grid barrier: make them visible to the async proxy, and order this
+        // warp's reads of the buffer before its refill
+        asm volatile("fence.proxy.async.global;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b),
+                     "r"(abytes + rbytes + vbytes + obytes)
+                     : "memory");
+        if (abytes) bulk_copy(ws.adjs[buf], a.adj + ab, abytes, b, pol);
+        bulk_copy(ws.rows[buf], row_of<S>(a, v0), rbytes, b, evict_normal_policy());
+        bulk_copy(ws.vbuf[buf], a.vinfo + vb, vbytes, b, evict_normal_policy());
+        bulk_copy(ws.obuf[buf], a.offs + obb, obytes, b, evict_normal_policy());
+    }
+}
+
 // Runs one sweep: the grid walks the work items, item i being
 // list[(start + i) % ring] (or tile i when list is null); with x.split > 1
 // each item is cut into x.split parts handed to different warps.  CTA b owns
@@ -721,10 +878,18 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
 // working instead of waiting at the sweep's barrier.
 // With no list and a range table, item i is tile ranges[r].x + (i - ranges[r].y)
 // for the last range r with ranges[r].y <= i (nranges ranges, increasing .y).
+// Each warp keeps a pipeline of drawn items: the tile being worked on, the
+// next one (its adjacency, rows, degree words and row starts in flight to the
+// other buffer), the one after (descriptor loaded) and one more (list entry
+// loaded).
+// pstate holds the warp's buffer phases (bits 0, 1) and next buffer (bit 2)
+// across sweeps.  A copy that does not arrive within wait_ns sets
+// BCG_ERR_TIMEOUT and ends the warp's part of the sweep.
 template <int S, bool EXT>
 __device__ __forceinline__ void run_sweep(const BatchArgs &a, Smem<S> &sm, const SweepCtx &x, const uint32_t *list,
-                          unsigned long long start, uint32_t nwork, unsigned long long ring,
-                          const uint2 *ranges = nullptr, uint32_t nranges = 0) {
+                                          unsigned long long start, uint32_t nwork, unsigned long long ring,
+                                          uint32_t &pstate, unsigned long long wait_ns,
+                                          const uint2 *ranges = nullptr, uint32_t nranges = 0) {
     const unsigned wid = threadIdx.x >> 5;
     WarpSmem<S> &ws = sm.w[wid];
     if ((threadIdx.x & 31) == 0) {
@@ -734,9 +899,10 @@ __device__ __forceinline__ void run_sweep(const BatchArgs &a, Smem<S> &sm, const
         for (int q = 0; q < 2 + 3 * S; ++q) ws.cnt[q] = 0ull;
     }
     __syncwarp();
-    const unsigned long long nitems = (unsigned long long)nwork * x.split;
-    auto item_tile = [&](unsigned long long it) -> uint32_t {
-        const uint32_t i = (uint32_t)(it / x.split);
+    // item numbers fit 32 bits: a sweep's work list holds at most 2^31 tiles
+    const uint32_t nitems = nwork * x.split;
+    auto item_tile = [&](uint32_t it) -> uint32_t {
+        const uint32_t i = it / x.split;
         if (list) return list[(start + i) % ring];
         if (!ranges) return i;
         uint32_t lo = 0, hi = nranges;
@@ -748,34 +914,59 @@ __device__ __forceinline__ void run_sweep(const BatchArgs &a, Smem<S> &sm, const
         return r.x + (i - r.y);
     };
     const unsigned long long G = gridDim.x;
-    auto grab = [&]() -> unsigned long long {
-        unsigned long long c = 0;
+    auto grab = [&]() -> uint32_t {
+        uint32_t c = 0;
         if ((threadIdx.x & 31) == 0) c = atomicAdd(&sm.next, 1u);
         c = __shfl_sync(0xffffffffu, c, 0);
-        return blockIdx.x + c * G;
+        const unsigned long long it = blockIdx.x + (unsigned long long)c * G;
+        return it < nitems ? (uint32_t)it : nitems;
     };
-    // software prefetch: each warp holds two drawn items; the descriptor of the
-    // next one and the list entry of the one after are loaded an iteration early
-    unsigned long long it = grab();
-    unsigned long long it2 = (it < nitems) ? grab() : nitems;
-    uint32_t ti1 = (it < nitems) ? item_tile(it) : 0u;
-    uint32_t ti2 = (it2 < nitems) ? item_tile(it2) : 0u;
-    Tile T1{};
-    if (it < nitems) T1 = a.tiles[ti1];
-    while (it < nitems) {
-        const uint32_t part = (uint32_t)(it % x.split);
-        const uint32_t ti = ti1;
-        const Tile T = T1;
-        const unsigned long long it_next = it2;
-        if (it2 < nitems) T1 = a.tiles[ti2];
-        ti1 = ti2;
-        it2 = (it2 < nitems) ? grab() : nitems;
-        if (it2 < nitems) ti2 = item_tile(it2);
-        if (x.mode == kFwdPush) warp_tile<S, kFwdPush, EXT>(a, sm, ws, ti, T, part, x);
-        else if (x.mode == kFwdPull) warp_tile<S, kFwdPull, EXT>(a, sm, ws, ti, T, 0, x);
-        else warp_tile<S, kBwd, EXT>(a, sm, ws, ti, T, 0, x);
-        __syncwarp();
-        it = it_next;
+    const unsigned long long pol = evict_first_policy();
+    uint32_t itA = grab();
+    if (itA < nitems) {
+        int buf = (pstate >> 2) & 1;
+        uint32_t tiA = item_tile(itA);
+        uint32_t twA = tile_word(a.tiles, tiA);
+        uint32_t itB = grab();
+        uint32_t tiB = (itB < nitems) ? item_tile(itB) : 0u;
+        tile_fetch<S>(a, ws, buf, twA, pol);
+        uint32_t twB = (itB < nitems) ? tile_word(a.tiles, tiB) : 0u;
+        uint32_t itC = (itB < nitems) ? grab() : nitems;
+        uint32_t tiC = (itC < nitems) ? item_tile(itC) : 0u;
+        for (;;) {
+            if (itB < nitems) tile_fetch<S>(a, ws, buf ^ 1, twB, pol);
+            const uint32_t twC = (itC < nitems) ? tile_word(a.tiles, tiC) : 0u;
+            const uint32_t itD = (itC < nitems) ? grab() : nitems;
+            const uint32_t tiD = (itD < nitems) ? item_tile(itD) : 0u;
+            const bool got = mbar_wait(&ws.mbar[buf], (pstate >> buf) & 1u, wait_ns);
+            pstate ^= 1u << buf;
+            if (!__all_sync(0xffffffffu, got)) {
+                // a copy that never arrived: record it, give the copy still in
+                // flight one more bounded wait, and leave the sweep
+                if ((threadIdx.x & 31) == 0) set_error(a.ctrl, BCG_ERR_TIMEOUT);
+                if (itB < nitems) {
+                    mbar_wait(&ws.mbar[buf ^ 1], (pstate >> (buf ^ 1)) & 1u, wait_ns);
+                    pstate ^= 1u << (buf ^ 1);
+                }
+                __syncwarp();
+                pstate = (pstate & 3u) | ((uint32_t)buf << 2);
+                break;
+            }
+            const Tile TA = tile_unpack(twA);
+            const uint32_t part = itA % x.split;
+            if (x.mode == kFwdPush) warp_tile<S, kFwdPush, EXT>(a, sm, ws, tiA, TA, part, x, buf);
+            else if (x.mode == kFwdPull) warp_tile<S, kFwdPull, EXT>(a, sm, ws, tiA, TA, 0, x, buf);
+            else warp_tile<S, kBwd, EXT>(a, sm, ws, tiA, TA, 0, x, buf);
+            __syncwarp();
+            buf ^= 1;
+            if (itB >= nitems) {
+                pstate = (pstate & 3u) | ((uint32_t)buf << 2);
+                break;
+            }
+            itA = itB; tiA = tiB; twA = twB;
+            itB = itC; tiB = tiC; twB = twC;
+            itC = itD; tiC = tiD;
+        }
     }
     if (x.mode != kBwd) {
         const uint32_t cnt = ws.napp;
@@ -798,7 +989,7 @@ __device__ __forceinline__ void run_sweep(const BatchArgs &a, Smem<S> &sm, const
 
 template <int S, bool EXT>
 __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     Smem<S> &sm = *reinterpret_cast<Smem<S> *>(smem_raw);
     constexpr int R = RowGeom<S>::kBytes;
     Ctrl *c = a.ctrl;
@@ -806,6 +997,16 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
     const unsigned long long wait_ns = c->wait_ns ? c->wait_ns : kDefaultWaitNs;
     const unsigned long long ring = 2ull * a.ntiles;
     const uint32_t total_warps = gridDim.x * kWarps;
+    {
+        WarpSmem<S> &ws = sm.w[threadIdx.x >> 5];
+        if ((threadIdx.x & 31) == 0) {
+            mbar_init(&ws.mbar[0]);
+            mbar_init(&ws.mbar[1]);
+            mbar_init_fence();
+        }
+        __syncwarp();
+    }
+    uint32_t pstate = 0;  // this warp's tile-buffer phases and next buffer
 
     const bool packed = a.xbeg != nullptr;
     for (uint32_t b = 0; b < a.nbatch; ++b) {
@@ -955,11 +1156,11 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
             if (x.mode == kFwdPull) {
                 walked = uall ? (packed ? a.xtiles[b] : a.ntiles) : ulen;
                 const bool ranged = uall && packed;
-                run_sweep<S, EXT>(a, sm, x, uall ? nullptr : a.ulist, ustart, walked, ring,
-                             ranged ? a.xrange + a.xrbeg[b] : nullptr, ranged ? a.xrbeg[b + 1] - a.xrbeg[b] : 0u);
+                run_sweep<S, EXT>(a, sm, x, uall ? nullptr : a.ulist, ustart, walked, ring, pstate, wait_ns,
+                                  ranged ? a.xrange + a.xrbeg[b] : nullptr, ranged ? a.xrbeg[b + 1] - a.xrbeg[b] : 0u);
             } else {
                 walked = lc;
-                run_sweep<S, EXT>(a, sm, x, a.lists + lb, 0, lc, 0xFFFFFFFFull);
+                run_sweep<S, EXT>(a, sm, x, a.lists + lb, 0, lc, 0xFFFFFFFFull, pstate, wait_ns);
             }
             __syncthreads();
             if (threadIdx.x == 0) {
@@ -1001,11 +1202,17 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
         const uint32_t D = d;
 
         if (a.dbg_sigma) {
-            // single-slot debug run: copy sigma out before the backward pass
+            // debug run: copy every slot's levels and sigma out before the
+            // backward pass overwrites sigma
             for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < a.n;
                  v += (size_t)gridDim.x * blockDim.x) {
                 unsigned char *row = a.rows + v * R;
-                a.dbg_sigma[v] = (*lvl_at(row, 0) == kUnvisited) ? 0ull : *val_at<S>(row, 0);
+#pragma unroll
+                for (int k = 0; k < S; ++k) {
+                    const uint16_t L = *lvl_at(row, k);
+                    a.dbg_level[(size_t)k * a.n + v] = (L == kUnvisited) ? -1 : (int32_t)L;
+                    a.dbg_sigma[(size_t)k * a.n + v] = (L == kUnvisited) ? 0ull : *val_at<S>(row, k);
+                }
             }
             if (!grid_sync(c, nblk, wait_ns)) return;
         }
@@ -1031,7 +1238,7 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
             }
             if (threadIdx.x == 0) sm.next = 0;
             __syncthreads();
-            run_sweep<S, EXT>(a, sm, x, a.lists + lb, 0, lc, 0xFFFFFFFFull);
+            run_sweep<S, EXT>(a, sm, x, a.lists + lb, 0, lc, 0xFFFFFFFFull, pstate, wait_ns);
             if (!grid_sync(c, nblk, wait_ns)) return;
             trace(a, b, 3u, (uint32_t)dd, lc, 0);
         }

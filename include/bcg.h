@@ -126,6 +126,9 @@ typedef struct bcg_stats {
     double   kernel_ms;      /* device time of the BC kernels (CUDA events) */
     uint32_t extended_sigma; /* 1: path counts ran as extended-range numbers */
     uint32_t reserved;
+    uint64_t search_edges;   /* sum over roots of the undirected edges the search
+                                holds in the root's component (the pruned graph's
+                                edges: the work the sweeps actually read) */
 } bcg_stats;
 
 /* Number of CUDA devices visible (0 when none); never fails. */
@@ -188,6 +191,21 @@ int bcg_bc_csr(const uint32_t *offsets, const uint32_t *adj, uint32_t n,
  * Does not touch the bc accumulator. */
 int bcg_single_source(bcg_graph *g, uint32_t src, int32_t *level,
                       uint64_t *sigma, double *delta);
+
+/* Debug read-out of one real batch: runs the roots[0..nroots) (caller's ids,
+ * nroots <= width) as one batch of the given width (1, 3 or 6: the S of the
+ * sweep kernel's state rows) with root k in slot k, and copies out for every
+ * slot k and vertex v, at [k * n + v] in the caller's numbering, the BFS
+ * depth (-1 = unreachable), sigma, and delta.  The per-source state the
+ * reference keeps in lvl/sig/delta (setcuda + set_mlp_cuda + scan_col_mono2
+ * + scan_frt_mono, cuda_kernels.cu:471-599, 689-703, 1100-1119) for `width`
+ * sources at once.  Works in every pruning mode: with BCG_PRUNE_TREES the
+ * roots must be vertices of the searched 2-core (BCG_ERR_ARG otherwise) and
+ * pendant-tree vertices read -1 / 0 / 0.  Exact uint64 counts (overflow is
+ * BCG_ERR_OVERFLOW).  Does not touch the bc accumulator.  Any output may be
+ * NULL. */
+int bcg_debug_batch(bcg_graph *g, uint32_t width, const uint32_t *roots, uint32_t nroots,
+                    int32_t *level, uint64_t *sigma, double *delta);
 
 /* Pruning result of a graph created with BCG_PRUNE_DEGREE1: anchor[v] = the
  * vertex v was folded into, or v itself when v was kept; reach[v] = number of
@@ -322,15 +340,21 @@ int bcg_server_info(bcg_server *s, uint64_t *resident_bytes, uint64_t *admitted_
  * source list d_sources[nsrc] (degree-0 sources skipped, as bcg_run does),
  * written into the caller's device buffer d_bc[n] (ordered-pair sums like
  * bcg_get_bc): overwritten, or added to when accumulate != 0.  Work is
- * enqueued on `stream` (a cudaStream_t, NULL = default stream); the call
- * returns when it is done.
+ * enqueued on `stream` (a cudaStream_t, NULL = default stream).
+ *   - Synchronous: the call reads a status block back to the host and waits
+ *     for the stream before it returns, so it cannot be made while the
+ *     stream (or the device) is being captured into a CUDA graph.
  *   - Allocates no device memory and calls no allocating CUDA or library
  *     function: all scratch lives in one fixed static device array of about
  *     19 MiB per device, so n, nnz and nsrc are limited to the
  *     BCG_NOALLOC_MAX_* values above; larger inputs return BCG_ERR_RANGE.
+ *   - Path counts are exact uint64; when one overflows (graphs such as
+ *     large grids) the sweep is redone with extended-range counts from a
+ *     copy of d_bc saved before it, as bcg_run does with BCG_SIGMA_AUTO, so
+ *     d_bc is never left with a partial run in it.
  *   - The first call on each device (made with that device current) does the
  *     setup: it takes the array's address with cudaGetSymbolAddress, which
- *     loads the module.  Make that first call before any stream capture.
+ *     loads the module.
  *   - One scratch per device: calls that overlap on the same device (other
  *     threads or streams) race and must be serialised by the caller.
  *   - Invalid CSR or source ids are found on the device before the sweep

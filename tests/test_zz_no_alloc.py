@@ -11,6 +11,7 @@ import numpy as np
 import pytest
 
 import bcg
+import oracle
 from test_gpu_parity import assert_bc_close
 
 SPECS = {
@@ -75,6 +76,8 @@ def test_calls_in_a_row_match_handle_path():
         offs, adj, src, ref, dg = inputs[name]
         bc = dg.call()
         assert_bc_close(bc, ref, f"call {i} ({name})")
+        if i < 3:  # and against the oracle itself
+            assert_bc_close(bc, oracle.bc(offs, adj, src, nthreads=oracle.max_threads())[0], f"oracle {name}")
         if name in got:  # the same input again after other graphs used the scratch
             assert_bc_close(bc, got[name], f"repeat of {name}")
         got[name] = bc
@@ -130,3 +133,23 @@ def test_invalid_input_found_on_device():
     # the scratch is usable again right after a rejected call
     dg = _DevGraph(torch, offs, adj, src)
     assert_bc_close(dg.call(), ref, "after rejected calls")
+
+
+@pytest.mark.gpu
+def test_overflowing_counts_switch_to_extended():
+    """A 256 x 256 grid (65,536 vertices, at the vertex limit): path counts
+    reach about 2^505, past uint64.  The call must redo the sweep with
+    extended-range counts from the accumulators it saved, so an accumulating
+    call adds exactly one run's worth on top of what d_bc held."""
+    torch = pytest.importorskip("torch")
+    offs, adj = bcg.generate("grid:w=256,h=256,drop=0.0,seed=1")
+    n = len(offs) - 1
+    assert n == bcg.NOALLOC_MAX_VERTICES
+    src = np.array([0, 255, 32768, 40000, 65535, 12345], dtype=np.uint32)
+    ref, _ = oracle.bc_q(offs, adj, src, nthreads=oracle.max_threads())
+    dg = _DevGraph(torch, offs, adj, src)
+    dg.bc.fill_(1.0)
+    bc = dg.call(accumulate=True)
+    assert_bc_close(bc, ref + 1.0, "grid 256x256, accumulate on 1.0")
+    bc = dg.call(accumulate=False)
+    assert_bc_close(bc, ref, "grid 256x256, overwrite")
