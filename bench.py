@@ -330,9 +330,10 @@ def run_serve(args, rank, world):
     loop: the pool resident as one bcg_graph per graph, each request in
     arrival order as bcg_reset_bc + bcg_run(sources) + bcg_get_bc; its Poisson
     latencies replay the measured service times through a FIFO queue.
-    Served: bcg_server (HBM budget 150 GB); throughput with every request
-    queued at once, latency from a real-time replay of Poisson arrivals at
-    half the served throughput.  One GPU (replicas only)."""
+    Served: bcg_server (HBM budget 150 GB), a client thread submitting while
+    the serving thread steps; throughput with every request arriving at once,
+    latency from a real-time replay of Poisson arrivals at half the served
+    throughput.  One GPU (replicas only)."""
     import numpy as np
     import torch
 
@@ -381,24 +382,32 @@ def run_serve(args, rank, world):
     budget = 150 * 10**9
 
     def serve(arrivals):
+        """Requests are submitted by a client thread at their arrival times
+        while this thread keeps the server stepping (bcg_server_step never
+        waits for the GPU, so arrivals are admitted while waves run)."""
         done_at = {}
         S = bcg.Server(pool, budget, args.wave_batches)
         ids = [None] * len(reqs)
         results = {}
         t_start = time.perf_counter()
-        nxt = 0
+
+        def client():
+            for i, (g, src) in enumerate(reqs):
+                delay = arrivals[i] - (time.perf_counter() - t_start)
+                if delay > 0:
+                    time.sleep(delay)
+                ids[i] = S.submit(g, src)
+
+        th = threading.Thread(target=client)
+        th.start()
         while len(done_at) < len(reqs):
-            now = time.perf_counter() - t_start
-            while nxt < len(reqs) and arrivals[nxt] <= now:
-                g, src = reqs[nxt]
-                ids[nxt] = S.submit(g, src)
-                nxt += 1
-            if nxt == len(done_at) and nxt < len(reqs):
-                time.sleep(max(0.0, min(0.001, arrivals[nxt] - now)))
-                continue
-            for rid in S.step():
+            got = S.step()
+            for rid in got:
                 done_at[rid] = time.perf_counter() - t_start
                 results[rid] = S.result(rid)
+            if not got:
+                time.sleep(0.0002)
+        th.join()
         info = S.info()
         S.close()
         lat = [done_at[ids[i]] - arrivals[i] for i in range(len(reqs))]

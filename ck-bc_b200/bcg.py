@@ -123,6 +123,7 @@ SIGNATURES = {
     "bcg_server_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "bcg_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, _u32p, ctypes.c_uint64, _u64p]),
     "bcg_server_step": (ctypes.c_int, [ctypes.c_void_p, _u64p, ctypes.c_uint32, _u32p]),
+    "bcg_server_wait": (ctypes.c_int, [ctypes.c_void_p, _u64p, ctypes.c_uint32, _u32p]),
     "bcg_server_result": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, _f64p]),
     "bcg_server_info": (ctypes.c_int, [ctypes.c_void_p, _u64p, _u64p, _u32p, _u32p, _u64p]),
     "bcg_bc_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64,
@@ -403,8 +404,10 @@ class Batch:
 
 class Server:
     """Resident pool of graphs serving BC requests with continuous batching:
-    submit() queues, step() admits what fits and runs one wave, result()
-    returns a finished request's bc."""
+    submit() queues (from any thread), step() retires finished waves, admits
+    what fits and keeps the next waves queued without waiting for the GPU,
+    wait() does the same after the oldest wave in flight has finished,
+    result() returns a finished request's bc."""
 
     def __init__(self, graphs, budget_bytes: int, wave_batches: int = 64):
         self._keep = [(np.ascontiguousarray(o, dtype=np.uint32), np.ascontiguousarray(a, dtype=np.uint32))
@@ -453,6 +456,12 @@ class Server:
         ids = (ctypes.c_uint64 * cap)()
         nd = ctypes.c_uint32()
         _check(lib().bcg_server_step(self.h, ids, cap, ctypes.byref(nd)))
+        return [ids[i] for i in range(nd.value)]
+
+    def wait(self, cap: int = 4096):
+        ids = (ctypes.c_uint64 * cap)()
+        nd = ctypes.c_uint32()
+        _check(lib().bcg_server_wait(self.h, ids, cap, ctypes.byref(nd)))
         return [ids[i] for i in range(nd.value)]
 
     def result(self, rid: int) -> np.ndarray:

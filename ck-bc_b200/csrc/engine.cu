@@ -629,6 +629,7 @@ int enqueue_packed(bcg_graph *g, const PackedRun &p, uint32_t S, cudaStream_t st
     a.xtiles = p.xtiles;
     a.xrbeg = p.xrbeg;
     a.xrange = p.xrange;
+    a.xout = p.xout;
     int grid = 0;
     return launch_sweep((int)S, a, st, &grid);
 }

@@ -99,6 +99,15 @@ struct RootStat {
     unsigned int pad;
 };
 
+// Where the dependencies of one graph's slots in one packed batch go (served
+// waves): slot k's delta of vertex v is added to out[k][v - base] (nullptr:
+// slot k holds no root of that graph in that batch).
+struct SlotOut {
+    double *out[6];
+    uint32_t base;
+    uint32_t pad;
+};
+
 struct BatchArgs {
     uint32_t n;             // vertices with state rows a sweep may touch (the tiles' range)
     const uint32_t *offs;   // CSR row starts (n+1); pruned lists start here too
@@ -156,6 +165,9 @@ struct BatchArgs {
     const uint32_t *xtiles;
     const uint32_t *xrbeg;
     const uint2 *xrange;
+    // served waves: xout[q] routes the slots of range q (ranges of a batch
+    // sorted by first tile); nullptr: dependencies go to bc as usual
+    const SlotOut *xout;
 };
 
 }  // namespace bcg

@@ -94,6 +94,7 @@ struct PackedRun {
     const unsigned long long *xpf, *xpu;
     const uint32_t *xtiles, *xrbeg;
     const uint2 *xrange;
+    const bcg::SlotOut *xout;  // nullptr: dependencies into the union's bc
     uint32_t nbatch;
     RootStat *rstat;  // nbatch * S per-slot totals
 };

@@ -7,23 +7,30 @@
 // asks for the BC of one graph over a list of sources (or all of its
 // vertices); its result buffer (one double per vertex of the graph) is
 // allocated when it is admitted, FIFO, while the pool plus the admitted
-// buffers fit the budget.  Each graph serves its admitted requests in order.
+// buffers fit the budget.
 //
-// bcg_server_step runs one wave: every graph with an admitted request
-// advances its first request by a chunk of up to wave_batches * S sources, all
-// of them packed into one persistent launch (component-packed batches: a
-// graph's sources fill the S slots of successive batches, graphs share the
-// batches; S is 6 while the active graphs' 64-byte state rows fit 64 MB, as
-// in bcg_run, else 3).  The first pull of a batch walks only the tile ranges of the
-// graphs active in it.  After the launch a drain kernel adds each active
-// graph's slice of the union's bc into its request's buffer and clears the
-// slice.  A request that arrives while a wave runs joins the next one, so the
-// GPU always works on every admitted request at once, and large requests do
-// not hold small ones back for longer than one wave.  Every source of a
-// request adds the same dependencies alone or in a mix; only the grouping of
-// those floating-point sums into waves may differ with the wave width.
+// Waves.  A wave is one persistent launch of packed batches (component-packed:
+// the graphs active in the wave share every batch, each graph filling the S
+// slots with its own sources).  Each graph takes up to wave_batches * S of
+// the not yet scheduled sources of ALL its admitted requests, oldest request
+// first, so requests on the same graph share the adjacency passes of a
+// batch.  The sweep kernel adds each slot's dependencies straight into the
+// buffer of the request that owns the slot's source (SlotOut routing), one
+// slot after the other: a request's sources reach its buffer in its own
+// source order however they are packed, so its result is bitwise the same
+// alone or in any mix.  S is 6 while the active graphs' 64-byte state rows
+// fit 64 MB (they then stay in L2), else 3.
+//
+// Continuity.  bcg_server_step never waits for the GPU: it retires the waves
+// that have finished (their requests become done), admits what fits, and
+// keeps up to two waves queued on the server's stream, so the next wave is
+// planned and enqueued while the current one runs and the device does not
+// idle between waves.  Every entry point takes the server's lock, so other
+// threads may submit while a wave is on the GPU: such a request is admitted
+// at once if its buffer fits and joins the next wave that is planned.
 #include <algorithm>
 #include <deque>
+#include <mutex>
 #include <unordered_map>
 #include <vector>
 
@@ -37,35 +44,31 @@ namespace {
 struct Req {
     uint32_t graph = 0;
     std::vector<uint32_t> src;  // union ids of the request's non-isolated sources, in order
-    size_t next = 0;            // sources already run
+    size_t sched = 0;           // sources already placed in a wave
     double *d_out = nullptr;    // one accumulator per vertex of the graph (from admission on)
     size_t bytes = 0;
     bool done = false;
 };
 
-struct DrainItem {
-    double *out;
-    uint32_t base;
-    uint32_t n;
-};
-
-// out[v] += bc[base + v]; bc[base + v] = 0 for every listed graph slice.
-__global__ void k_drain(const DrainItem *__restrict__ items, uint32_t nitems, double *__restrict__ bc) {
-    for (uint32_t it = blockIdx.y; it < nitems; it += gridDim.y) {
-        const DrainItem d = items[it];
-        for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < d.n; v += gridDim.x * blockDim.x) {
-            double *p = bc + d.base + v;
-            d.out[v] += *p;
-            *p = 0.0;
-        }
-    }
-}
-
 size_t up16(size_t x) { return (x + 15) & ~size_t(15); }
+
+constexpr int kInFlight = 2;  // waves queued on the stream at once
 
 }  // namespace
 
+// One enqueued wave: its schedule buffers, completion event, error flags and
+// the requests whose last source it holds.
+struct ServeWave {
+    unsigned char *h_blob = nullptr, *d_blob = nullptr;
+    RootStat *d_rstat = nullptr;
+    int *h_flags = nullptr;  // Ctrl::error, Ctrl::overflow after the wave (pinned)
+    cudaEvent_t ev = nullptr;
+    bool busy = false;
+    std::vector<uint64_t> finishing;
+};
+
 struct bcg_server {
+    std::mutex mu;
     bcg_graph *g = nullptr;
     uint32_t ngraphs = 0;
     std::vector<uint32_t> base, gn, order, hdeg;
@@ -76,16 +79,16 @@ struct bcg_server {
     std::unordered_map<uint64_t, Req> reqs;
     uint64_t next_id = 1;
     std::deque<uint64_t> pending;
-    std::vector<std::deque<uint64_t>> queue;  // per graph: admitted requests in order
+    std::vector<std::deque<uint64_t>> queue;  // per graph: admitted requests with unscheduled sources, in order
     std::deque<uint64_t> done;                // finished, not yet reported
-    // wave schedule: one device region and one pinned staging copy, sized for
-    // the largest wave (wave_batches batches, every graph active)
+    // wave schedule layout (one region per wave slot)
     size_t off_xbeg = 0, off_xroots = 0, off_xslot = 0, off_xpf = 0, off_xpu = 0, off_xtiles = 0, off_xrbeg = 0,
-           off_xrange = 0, off_drain = 0, blob_bytes = 0;
-    unsigned char *d_blob = nullptr, *h_blob = nullptr;
-    RootStat *d_rstat = nullptr;
-    cudaStream_t stream = nullptr;
+           off_xrange = 0, off_xout = 0, blob_bytes = 0;
+    ServeWave slot[kInFlight];
+    std::deque<int> inflight;  // wave slots in launch order
+    cudaStream_t stream = nullptr, result_stream = nullptr;
     uint64_t waves = 0;
+    int sticky_error = BCG_OK;  // a failed wave leaves the server unusable
 };
 
 namespace {
@@ -102,7 +105,7 @@ namespace {
 // tiles and their lists).
 uint64_t pool_bytes(const bcg_graph *g, uint32_t S) {
     const uint64_t n = g->n, t = g->ntiles;
-    return 4 * (n + 1) + 4 * (g->nnz + 4) + 8 * n /*vinfo*/ + 8 * n /*bc*/ + (uint64_t)row_bytes((int)S) * n +
+    return 4 * (n + 5) + 4 * (g->nnz + 4) + 8 * (n + 4) /*vinfo*/ + 8 * n /*bc*/ + (uint64_t)row_bytes((int)S) * n +
            32 * t + 4 * n /*tile_of*/ + 4 * t /*tmark*/ + 8 * t /*ring*/ + 4ull * S * (n + t) /*lists*/ +
            8ull * (kMaxLevel + 3);
 }
@@ -117,6 +120,176 @@ int admit(bcg_server *s) {
         s->admitted += r.bytes;
         s->queue[r.graph].push_back(s->pending.front());
         s->pending.pop_front();
+    }
+    return BCG_OK;
+}
+
+// Retires the finished waves at the front of the queue (wait: block for the
+// oldest one first).
+int retire(bcg_server *s, bool wait) {
+    while (!s->inflight.empty()) {
+        ServeWave &w = s->slot[s->inflight.front()];
+        if (wait) {
+            CKS(cudaEventSynchronize(w.ev));
+            wait = false;
+        } else {
+            const cudaError_t q = cudaEventQuery(w.ev);
+            if (q == cudaErrorNotReady) break;
+            if (q != cudaSuccess) return set_error(BCG_ERR_CUDA, "wave event: %s", cudaGetErrorString(q));
+        }
+        if (w.h_flags[1] || w.h_flags[0] == BCG_ERR_OVERFLOW) {
+            s->sticky_error = BCG_ERR_OVERFLOW;
+            return set_error(BCG_ERR_OVERFLOW, "a shortest-path count exceeded 2^64 in a served wave");
+        }
+        if (w.h_flags[0]) {
+            s->sticky_error = w.h_flags[0];
+            return set_error(w.h_flags[0], "device reported error %d in a served wave", w.h_flags[0]);
+        }
+        for (uint64_t rid : w.finishing) {
+            s->reqs[rid].done = true;
+            s->done.push_back(rid);
+        }
+        w.finishing.clear();
+        w.busy = false;
+        s->inflight.pop_front();
+    }
+    return BCG_OK;
+}
+
+// Plans the next wave from the admitted requests' unscheduled sources and
+// enqueues it on the server's stream.  *launched = false when there is no
+// work (or no free wave slot).
+int enqueue_wave(bcg_server *s, bool *launched) {
+    *launched = false;
+    int wi = -1;
+    for (int i = 0; i < kInFlight; ++i)
+        if (!s->slot[i].busy) { wi = i; break; }
+    if (wi < 0) return BCG_OK;
+    const uint32_t G = s->ngraphs, W = s->wave_batches;
+    // the graphs with work, and their active vertices (for the width rule)
+    std::vector<uint32_t> act;
+    uint64_t act_n = 0;
+    for (uint32_t gi = 0; gi < G; ++gi) {
+        if (s->queue[gi].empty()) continue;
+        act.push_back(gi);
+        act_n += s->gn[gi];
+    }
+    if (act.empty()) return BCG_OK;
+    const uint32_t S = (act_n * (uint64_t)row_bytes(6) <= (64ull << 20)) ? 6u : 3u;
+    // each active graph's list for this wave: (source, request) pairs, its
+    // admitted requests' unscheduled sources oldest request first
+    struct Pick { uint32_t v; uint64_t rid; };
+    std::vector<std::vector<Pick>> picks(act.size());
+    ServeWave &w = s->slot[wi];
+    w.finishing.clear();
+    uint32_t nb = 0;
+    for (size_t a = 0; a < act.size(); ++a) {
+        auto &q = s->queue[act[a]];
+        const size_t cap = (size_t)W * S;
+        while (!q.empty() && picks[a].size() < cap) {
+            Req &r = s->reqs[q.front()];
+            const size_t take = std::min(cap - picks[a].size(), r.src.size() - r.sched);
+            for (size_t j = 0; j < take; ++j) picks[a].push_back(Pick{r.src[r.sched + j], q.front()});
+            r.sched += take;
+            if (r.sched == r.src.size()) {
+                w.finishing.push_back(q.front());
+                q.pop_front();
+            }
+        }
+        nb = std::max<uint32_t>(nb, (uint32_t)((picks[a].size() + S - 1) / S));
+    }
+    // requests with no source left to run (all of degree 0) finish with this wave
+    unsigned char *h = w.h_blob;
+    auto *xbeg = reinterpret_cast<uint32_t *>(h + s->off_xbeg);
+    auto *xroots = reinterpret_cast<uint32_t *>(h + s->off_xroots);
+    auto *xslot = h + s->off_xslot;
+    auto *xpf = reinterpret_cast<unsigned long long *>(h + s->off_xpf);
+    auto *xpu = reinterpret_cast<unsigned long long *>(h + s->off_xpu);
+    auto *xtiles = reinterpret_cast<uint32_t *>(h + s->off_xtiles);
+    auto *xrbeg = reinterpret_cast<uint32_t *>(h + s->off_xrbeg);
+    auto *xrange = reinterpret_cast<uint2 *>(h + s->off_xrange);
+    auto *xout = reinterpret_cast<SlotOut *>(h + s->off_xout);
+    uint32_t nr = 0, nrange = 0;
+    xbeg[0] = 0;
+    xrbeg[0] = 0;
+    for (uint32_t i = 0; i < nb; ++i) {
+        xpf[i] = xpu[i] = 0;
+        uint32_t cum = 0;
+        // act is in caller-graph order and the union keeps that order, so the
+        // batch's ranges ascend by first tile (the kernel searches them)
+        for (size_t a = 0; a < act.size(); ++a) {
+            const size_t j0 = (size_t)i * S;
+            if (j0 >= picks[a].size()) continue;
+            const uint32_t gi = act[a];
+            SlotOut o{};
+            o.base = s->base[gi];
+            for (uint32_t k = 0; k < S && j0 + k < picks[a].size(); ++k) {
+                const Pick &pk = picks[a][j0 + k];
+                xroots[nr] = pk.v;
+                xslot[nr] = (unsigned char)k;
+                ++nr;
+                xpf[i] += s->hdeg[pk.v];
+                xpu[i] += s->gnnz[gi] - s->hdeg[pk.v];
+                o.out[k] = s->reqs[pk.rid].d_out;
+            }
+            xout[nrange] = o;
+            xrange[nrange++] = make_uint2(s->grange[gi].x, cum);
+            cum += s->grange[gi].y - s->grange[gi].x;
+        }
+        xbeg[i + 1] = nr;
+        xrbeg[i + 1] = nrange;
+        xtiles[i] = cum;
+    }
+    if (nb) {
+        CKS(cudaMemcpyAsync(w.d_blob, w.h_blob, s->blob_bytes, cudaMemcpyHostToDevice, s->stream));
+        unsigned char *d = w.d_blob;
+        PackedRun p{};
+        p.xbeg = reinterpret_cast<const uint32_t *>(d + s->off_xbeg);
+        p.xroots = reinterpret_cast<const uint32_t *>(d + s->off_xroots);
+        p.xslot = d + s->off_xslot;
+        p.xpf = reinterpret_cast<const unsigned long long *>(d + s->off_xpf);
+        p.xpu = reinterpret_cast<const unsigned long long *>(d + s->off_xpu);
+        p.xtiles = reinterpret_cast<const uint32_t *>(d + s->off_xtiles);
+        p.xrbeg = reinterpret_cast<const uint32_t *>(d + s->off_xrbeg);
+        p.xrange = reinterpret_cast<const uint2 *>(d + s->off_xrange);
+        p.xout = reinterpret_cast<const SlotOut *>(d + s->off_xout);
+        p.nbatch = nb;
+        p.rstat = w.d_rstat;
+        int rc = enqueue_packed(s->g, p, S, s->stream);
+        if (rc) return rc;
+        // the wave's error flags, read by the host once its event has passed
+        CKS(cudaMemcpyAsync(w.h_flags, &s->g->d_ctrl->error, 2 * sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    } else {
+        w.h_flags[0] = w.h_flags[1] = 0;
+    }
+    CKS(cudaEventRecord(w.ev, s->stream));
+    w.busy = true;
+    s->inflight.push_back(wi);
+    ++s->waves;
+    *launched = true;
+    return BCG_OK;
+}
+
+// The common body of step and wait (lock held).
+int step_locked(bcg_server *s, bool wait, uint64_t *done_ids, uint32_t cap, uint32_t *ndone) {
+    *ndone = 0;
+    if (s->sticky_error) return set_error(s->sticky_error, "an earlier served wave failed (error %d)", s->sticky_error);
+    int rc = retire(s, wait && !s->inflight.empty());
+    if (rc) return rc;
+    rc = admit(s);
+    if (rc) return rc;
+    while ((int)s->inflight.size() < kInFlight) {
+        bool launched = false;
+        rc = enqueue_wave(s, &launched);
+        if (rc) {
+            s->sticky_error = rc;
+            return rc;
+        }
+        if (!launched) break;
+    }
+    while (!s->done.empty() && *ndone < cap) {
+        done_ids[(*ndone)++] = s->done.front();
+        s->done.pop_front();
     }
     return BCG_OK;
 }
@@ -165,6 +338,9 @@ int bcg_server_create(uint32_t ngraphs, const uint32_t *const *offsets, const ui
         s->grange[gi] = make_uint2(t0, t1);
         for (uint32_t v = 0; v < n[gi]; ++v) s->gnnz[gi] += s->hdeg[s->base[gi] + v];
     }
+    for (uint32_t gi = 1; gi < ngraphs; ++gi)
+        if (s->grange[gi].x < s->grange[gi - 1].x)
+            return fail(set_error(BCG_ERR_ARG, "the pool union does not keep the graphs in caller order"));
     rc = ensure_state(s->g, s->width);
     if (rc) return fail(rc);
     s->budget = hbm_budget_bytes;
@@ -172,7 +348,8 @@ int bcg_server_create(uint32_t ngraphs, const uint32_t *const *offsets, const ui
     if (s->resident > s->budget)
         return fail(set_error(BCG_ERR_OOM, "the resident pool needs %llu bytes, over the %llu-byte budget",
                               (unsigned long long)s->resident, (unsigned long long)s->budget));
-    // wave schedule regions
+    // wave schedule regions (a wave has at most wave_batches batches, each
+    // with every graph active)
     const size_t W = wave_batches, G = ngraphs, S = s->width, R = W * G * S;
     size_t o = 0;
     s->off_xbeg = o; o += up16((W + 1) * 4);
@@ -183,14 +360,21 @@ int bcg_server_create(uint32_t ngraphs, const uint32_t *const *offsets, const ui
     s->off_xtiles = o; o += up16(W * 4);
     s->off_xrbeg = o; o += up16((W + 1) * 4);
     s->off_xrange = o; o += up16(W * G * 8);
-    s->off_drain = o; o += up16(G * sizeof(DrainItem));
+    s->off_xout = o; o += up16(W * G * sizeof(SlotOut));
     s->blob_bytes = o;
     cudaError_t e;
     if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess ||
-        (e = cudaMalloc(&s->d_blob, o)) != cudaSuccess || (e = cudaMallocHost(&s->h_blob, o)) != cudaSuccess ||
-        (e = cudaMalloc(&s->d_rstat, W * S * sizeof(RootStat))) != cudaSuccess)
-        return fail(set_error(BCG_ERR_CUDA, "server buffers: %s", cudaGetErrorString(e)));
-    s->resident += o + W * S * sizeof(RootStat);
+        (e = cudaStreamCreateWithFlags(&s->result_stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return fail(set_error(BCG_ERR_CUDA, "server streams: %s", cudaGetErrorString(e)));
+    for (int i = 0; i < kInFlight; ++i) {
+        ServeWave &w = s->slot[i];
+        if ((e = cudaMalloc(&w.d_blob, o)) != cudaSuccess || (e = cudaMallocHost(&w.h_blob, o)) != cudaSuccess ||
+            (e = cudaMalloc(&w.d_rstat, W * S * sizeof(RootStat))) != cudaSuccess ||
+            (e = cudaMallocHost(&w.h_flags, 2 * sizeof(int))) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&w.ev, cudaEventDisableTiming)) != cudaSuccess)
+            return fail(set_error(BCG_ERR_CUDA, "server buffers: %s", cudaGetErrorString(e)));
+        s->resident += o + W * S * sizeof(RootStat);
+    }
     *out = s;
     return BCG_OK;
 }
@@ -198,14 +382,23 @@ int bcg_server_create(uint32_t ngraphs, const uint32_t *const *offsets, const ui
 int bcg_server_destroy(bcg_server *s) {
     clear_error();
     if (!s) return set_error(BCG_ERR_ARG, "null handle");
-    if (s->stream) cudaStreamSynchronize(s->stream);
-    for (auto &kv : s->reqs)
-        if (kv.second.d_out) cudaFree(kv.second.d_out);
-    cudaFree(s->d_blob);
-    cudaFree(s->d_rstat);
-    if (s->h_blob) cudaFreeHost(s->h_blob);
-    if (s->stream) cudaStreamDestroy(s->stream);
-    if (s->g) bcg_graph_destroy(s->g);
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        if (s->stream) cudaStreamSynchronize(s->stream);
+        if (s->result_stream) cudaStreamSynchronize(s->result_stream);
+        for (auto &kv : s->reqs)
+            if (kv.second.d_out) cudaFree(kv.second.d_out);
+        for (ServeWave &w : s->slot) {
+            cudaFree(w.d_blob);
+            cudaFree(w.d_rstat);
+            if (w.h_blob) cudaFreeHost(w.h_blob);
+            if (w.h_flags) cudaFreeHost(w.h_flags);
+            if (w.ev) cudaEventDestroy(w.ev);
+        }
+        if (s->stream) cudaStreamDestroy(s->stream);
+        if (s->result_stream) cudaStreamDestroy(s->result_stream);
+        if (s->g) bcg_graph_destroy(s->g);
+    }
     delete s;
     return BCG_OK;
 }
@@ -213,6 +406,7 @@ int bcg_server_destroy(bcg_server *s) {
 int bcg_server_submit(bcg_server *s, uint32_t graph, const uint32_t *sources, uint64_t nsrc, uint64_t *id) {
     clear_error();
     if (!s || !id) return set_error(BCG_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> lock(s->mu);
     if (graph >= s->ngraphs) return set_error(BCG_ERR_ARG, "graph %u >= %u graphs", graph, s->ngraphs);
     if (nsrc && !sources) return set_error(BCG_ERR_ARG, "null sources");
     Req r;
@@ -240,132 +434,41 @@ int bcg_server_submit(bcg_server *s, uint32_t graph, const uint32_t *sources, ui
 int bcg_server_step(bcg_server *s, uint64_t *done_ids, uint32_t cap, uint32_t *ndone) {
     clear_error();
     if (!s || !ndone || (cap && !done_ids)) return set_error(BCG_ERR_ARG, "null argument");
-    *ndone = 0;
-    int rc = admit(s);
-    if (rc) return rc;
-    const uint32_t G = s->ngraphs, W = s->wave_batches;
-    // the graphs active in this wave; the wave's width follows bcg_run's rule:
-    // 6 sources per batch while the active graphs' 64-byte state rows fit
-    // 64 MB (they then stay in L2), else 3
-    std::vector<uint32_t> act;  // caller graph ids
-    uint64_t act_n = 0;
-    for (uint32_t gi = 0; gi < G; ++gi) {
-        auto &q = s->queue[gi];
-        while (!q.empty() && s->reqs[q.front()].next >= s->reqs[q.front()].src.size()) {
-            s->reqs[q.front()].done = true;
-            s->done.push_back(q.front());
-            q.pop_front();
-        }
-        if (q.empty()) continue;
-        act.push_back(gi);
-        act_n += s->gn[gi];
+    std::lock_guard<std::mutex> lock(s->mu);
+    return step_locked(s, false, done_ids, cap, ndone);
+}
+
+int bcg_server_wait(bcg_server *s, uint64_t *done_ids, uint32_t cap, uint32_t *ndone) {
+    clear_error();
+    if (!s || !ndone || (cap && !done_ids)) return set_error(BCG_ERR_ARG, "null argument");
+    cudaEvent_t ev = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        if (!s->inflight.empty()) ev = s->slot[s->inflight.front()].ev;
     }
-    const uint32_t S = (act_n * (uint64_t)row_bytes(6) <= (64ull << 20)) ? 6u : 3u;
-    std::vector<size_t> c0, c1;  // the chunk each active graph runs in this wave
-    for (uint32_t gi : act) {
-        const Req &r = s->reqs[s->queue[gi].front()];
-        c0.push_back(r.next);
-        c1.push_back(std::min(r.src.size(), r.next + (size_t)W * S));
+    // wait without the lock, so other threads can submit meanwhile (the
+    // event stays valid: only this server's own waves re-record it)
+    if (ev) {
+        const cudaError_t e = cudaEventSynchronize(ev);
+        if (e != cudaSuccess) return set_error(BCG_ERR_CUDA, "waiting for a wave: %s", cudaGetErrorString(e));
     }
-    if (!act.empty()) {
-        uint32_t nb = 0;
-        for (size_t a = 0; a < act.size(); ++a) nb = std::max<uint32_t>(nb, (uint32_t)((c1[a] - c0[a] + S - 1) / S));
-        unsigned char *h = s->h_blob;
-        auto *xbeg = reinterpret_cast<uint32_t *>(h + s->off_xbeg);
-        auto *xroots = reinterpret_cast<uint32_t *>(h + s->off_xroots);
-        auto *xslot = h + s->off_xslot;
-        auto *xpf = reinterpret_cast<unsigned long long *>(h + s->off_xpf);
-        auto *xpu = reinterpret_cast<unsigned long long *>(h + s->off_xpu);
-        auto *xtiles = reinterpret_cast<uint32_t *>(h + s->off_xtiles);
-        auto *xrbeg = reinterpret_cast<uint32_t *>(h + s->off_xrbeg);
-        auto *xrange = reinterpret_cast<uint2 *>(h + s->off_xrange);
-        auto *drain = reinterpret_cast<DrainItem *>(h + s->off_drain);
-        uint32_t nr = 0, nrange = 0;
-        xbeg[0] = 0;
-        xrbeg[0] = 0;
-        for (uint32_t i = 0; i < nb; ++i) {
-            xpf[i] = xpu[i] = 0;
-            uint32_t cum = 0;
-            for (size_t a = 0; a < act.size(); ++a) {
-                const size_t j0 = c0[a] + (size_t)i * S;
-                if (j0 >= c1[a]) continue;
-                const uint32_t gi = act[a];
-                const Req &r = s->reqs[s->queue[gi].front()];
-                for (uint32_t k = 0; k < S && j0 + k < c1[a]; ++k) {
-                    const uint32_t v = r.src[j0 + k];
-                    xroots[nr] = v;
-                    xslot[nr] = (unsigned char)k;
-                    ++nr;
-                    xpf[i] += s->hdeg[v];
-                    xpu[i] += s->gnnz[gi] - s->hdeg[v];
-                }
-                xrange[nrange++] = make_uint2(s->grange[gi].x, cum);
-                cum += s->grange[gi].y - s->grange[gi].x;
-            }
-            xbeg[i + 1] = nr;
-            xrbeg[i + 1] = nrange;
-            xtiles[i] = cum;
-        }
-        for (size_t a = 0; a < act.size(); ++a) {
-            const uint32_t gi = act[a];
-            drain[a] = DrainItem{s->reqs[s->queue[gi].front()].d_out, s->base[gi], s->gn[gi]};
-        }
-        CKS(cudaMemcpyAsync(s->d_blob, s->h_blob, s->blob_bytes, cudaMemcpyHostToDevice, s->stream));
-        unsigned char *d = s->d_blob;
-        PackedRun p{};
-        p.xbeg = reinterpret_cast<const uint32_t *>(d + s->off_xbeg);
-        p.xroots = reinterpret_cast<const uint32_t *>(d + s->off_xroots);
-        p.xslot = d + s->off_xslot;
-        p.xpf = reinterpret_cast<const unsigned long long *>(d + s->off_xpf);
-        p.xpu = reinterpret_cast<const unsigned long long *>(d + s->off_xpu);
-        p.xtiles = reinterpret_cast<const uint32_t *>(d + s->off_xtiles);
-        p.xrbeg = reinterpret_cast<const uint32_t *>(d + s->off_xrbeg);
-        p.xrange = reinterpret_cast<const uint2 *>(d + s->off_xrange);
-        p.nbatch = nb;
-        p.rstat = s->d_rstat;
-        rc = enqueue_packed(s->g, p, S, s->stream);
-        if (rc) return rc;
-        double *d_bc = nullptr;
-        rc = bcg_bc_device_ptr(s->g, &d_bc);
-        if (rc) return rc;
-        uint32_t maxn = 0;
-        for (uint32_t gi : act) maxn = std::max(maxn, s->gn[gi]);
-        const dim3 grid(std::min<uint32_t>((maxn + 255) / 256, 64u), (unsigned)act.size());
-        k_drain<<<grid, 256, 0, s->stream>>>(reinterpret_cast<const DrainItem *>(d + s->off_drain),
-                                             (uint32_t)act.size(), d_bc);
-        CKS(cudaGetLastError());
-        rc = check_ctrl(s->g, s->stream);
-        if (rc) return rc;
-        ++s->waves;
-        for (size_t a = 0; a < act.size(); ++a) {
-            const uint32_t gi = act[a];
-            const uint64_t rid = s->queue[gi].front();
-            Req &r = s->reqs[rid];
-            r.next = c1[a];
-            if (r.next >= r.src.size()) {
-                r.done = true;
-                s->done.push_back(rid);
-                s->queue[gi].pop_front();
-            }
-        }
-    }
-    while (!s->done.empty() && *ndone < cap) {
-        done_ids[(*ndone)++] = s->done.front();
-        s->done.pop_front();
-    }
-    return BCG_OK;
+    std::lock_guard<std::mutex> lock(s->mu);
+    return step_locked(s, false, done_ids, cap, ndone);
 }
 
 int bcg_server_result(bcg_server *s, uint64_t id, double *bc_host) {
     clear_error();
     if (!s || !bc_host) return set_error(BCG_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> lock(s->mu);
     auto it = s->reqs.find(id);
     if (it == s->reqs.end()) return set_error(BCG_ERR_ARG, "unknown request %llu", (unsigned long long)id);
     Req &r = it->second;
     if (!r.done) return set_error(BCG_ERR_ARG, "request %llu is not finished", (unsigned long long)id);
-    CKS(cudaMemcpyAsync(bc_host, r.d_out, r.bytes, cudaMemcpyDeviceToHost, s->stream));
-    CKS(cudaFreeAsync(r.d_out, s->stream));
-    CKS(cudaStreamSynchronize(s->stream));
+    // the last wave that wrote the buffer has completed: copy on the result
+    // stream, so later waves queued on the server's stream keep running
+    CKS(cudaMemcpyAsync(bc_host, r.d_out, r.bytes, cudaMemcpyDeviceToHost, s->result_stream));
+    CKS(cudaFreeAsync(r.d_out, s->result_stream));
+    CKS(cudaStreamSynchronize(s->result_stream));
     s->admitted -= r.bytes;
     s->reqs.erase(it);
     return BCG_OK;
@@ -375,8 +478,10 @@ int bcg_server_info(bcg_server *s, uint64_t *resident_bytes, uint64_t *admitted_
                     uint32_t *running, uint64_t *waves) {
     clear_error();
     if (!s) return set_error(BCG_ERR_ARG, "null handle");
+    std::lock_guard<std::mutex> lock(s->mu);
     uint32_t run = 0;
-    for (auto &q : s->queue) run += (uint32_t)q.size();
+    for (auto &kv : s->reqs)
+        if (kv.second.d_out && !kv.second.done) ++run;
     if (resident_bytes) *resident_bytes = s->resident;
     if (admitted_bytes) *admitted_bytes = s->admitted;
     if (pending) *pending = (uint32_t)s->pending.size();

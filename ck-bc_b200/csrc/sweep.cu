@@ -276,6 +276,7 @@ __device__ __forceinline__ Tile tile_unpack(uint32_t tw) {
 // Parameters of one sweep, identical in every warp.
 struct SweepCtx {
     int mode;
+    uint32_t b;          // batch
     uint32_t d, D;
     uint32_t key_next;   // tile mark of (batch, level d+1)
     uint32_t lb_next;    // list start of level d+1
@@ -794,6 +795,16 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
             const double reach = (double)vi.y;
             uint32_t ow[NW];
             own_row(ow);
+            // served waves: the slots' own result buffers for this tile's graph
+            const SlotOut *xo = nullptr;
+            if (a.xout) {
+                uint32_t lo = a.xrbeg[x.b], hi = a.xrbeg[x.b + 1];
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (a.xrange[mid].x <= ti) lo = mid; else hi = mid;
+                }
+                xo = a.xout + lo;
+            }
 #pragma unroll
             for (int k = 0; k < S; ++k) {
                 if (!((m >> k) & 1u)) continue;
@@ -811,10 +822,19 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
                     const double xo = (1.0 + delta) / sig;
                     *val_at<S>(vrow, k) = (unsigned long long)__double_as_longlong(xo);
                 }
-                if (d > 0) add += sm.mult[k] * delta;
+                if (d > 0) {
+                    if (xo) {
+                        // one add per slot, slots in order: a request's sources
+                        // reach its buffer in source order however they are packed
+                        double *o = xo->out[k];
+                        if (o) o[v - xo->base] += delta;
+                    } else {
+                        add += sm.mult[k] * delta;
+                    }
+                }
                 if (a.dbg_delta) a.dbg_delta[(size_t)k * a.n + v] = delta;
             }
-            if (d > 0) a.bc[a.ext ? a.ext[v] : v] += add;
+            if (d > 0 && !xo) a.bc[a.ext ? a.ext[v] : v] += add;
         }
     }
     if (MODE == kFwdPull) {
@@ -1131,6 +1151,7 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
         uint32_t lb = vload32(a.lbase), lc = vload32(a.lcnt);
         for (;;) {
             SweepCtx x;
+            x.b = b;
             x.mode = (!a.directed && (double)pf_cur >= (double)a.push_pull_ratio * (double)pu_cur) ? kFwdPull
                                                                                                     : kFwdPush;
             x.d = d;
@@ -1224,6 +1245,7 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
         uint32_t blb = vload32(a.lbase + D), blc = vload32(a.lcnt + D);
         for (int dd = (int)D; dd >= lowest; --dd) {
             SweepCtx x;
+            x.b = b;
             x.mode = kBwd;
             x.d = (uint32_t)dd;
             x.D = D;

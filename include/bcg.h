@@ -307,13 +307,21 @@ int bcg_server_destroy(bcg_server *s);
  * vertex of the graph, i.e. exact BC).  Sources of degree 0 are skipped, as
  * in bcg_run.  Its result buffer (8 bytes per vertex of the graph) is
  * allocated when the request is admitted, first come first served, while the
- * pool plus admitted buffers fit the budget. */
+ * pool plus admitted buffers fit the budget.  Every bcg_server_* call takes
+ * the server's lock: submit may be called from any thread, also while a wave
+ * is on the GPU (the request joins the next wave planned). */
 int bcg_server_submit(bcg_server *s, uint32_t graph, const uint32_t *sources, uint64_t nsrc,
                       uint64_t *id);
-/* Admits what fits, runs one wave (every graph with an admitted request
- * advances its oldest one by up to wave_batches * S sources, all in one
- * packed launch), and reports up to cap finished request ids. */
+/* Never waits for the GPU: retires the waves that have finished (their
+ * completed requests become done), admits what fits, and keeps up to two
+ * waves queued (a wave: every graph with admitted requests runs up to
+ * wave_batches * S of their unscheduled sources, oldest request first, all
+ * graphs in one packed launch), then reports up to cap finished request ids.
+ * A request's result is bitwise the same alone or in any mix. */
 int bcg_server_step(bcg_server *s, uint64_t *done_ids, uint32_t cap, uint32_t *ndone);
+/* bcg_server_step after waiting (without holding the lock) for the oldest
+ * wave in flight, if any. */
+int bcg_server_wait(bcg_server *s, uint64_t *done_ids, uint32_t cap, uint32_t *ndone);
 /* Copies a finished request's bc (ordered-pair sums, n doubles of its
  * graph) and releases its buffer and the request. */
 int bcg_server_result(bcg_server *s, uint64_t id, double *bc_host);
