@@ -182,14 +182,14 @@ static void graph_free(bcg_graph *g) {
     if (!g) return;
     int cur = -1;
     cudaGetDevice(&cur);
-    if (g->comp_job.valid()) g->comp_job.wait();
     if (cur != g->device) cudaSetDevice(g->device);
     cudaFree(g->d_offs); cudaFree(g->d_adj); cudaFree(g->d_vinfo);
     cudaFree(g->d_anchor); cudaFree(g->d_reach); cudaFree(g->d_bc);
     cudaFree(g->d_tiles); cudaFree(g->d_hub_acc); cudaFree(g->d_hub_cnt);
     cudaFree(g->d_tile_of); cudaFree(g->d_tmark); cudaFree(g->d_lists);
     cudaFree(g->d_lbase); cudaFree(g->d_lcnt); cudaFree(g->d_ulist); cudaFree(g->d_bc_save);
-    cudaFree(g->d_tree_acc);
+    tree_free(g);
+    cudaFree(g->d_vinfo_trees);
     cudaFree(g->d_ext);
     cudaFree(g->d_rows); cudaFree(g->d_ctrl);
     cudaFree(g->d_roots); cudaFree(g->d_pend); cudaFree(g->d_mult); cudaFree(g->d_rstat);
@@ -362,28 +362,16 @@ struct RunPlan {
     uint64_t tree_only = 0, tree_edges = 0, tree_verts = 0;
 };
 
-__global__ void k_add(uint32_t n, double *__restrict__ bc, const double *__restrict__ x) {
-    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v < n) bc[v] += x[v];
-}
-
 // Trees mode: the closed-form bc of the tree vertices (and the anchors' tree
 // terms) for this run's sources, added on the device after the search.
 static int add_tree_terms(bcg_graph *g, const uint32_t *src, uint64_t nsrc, const RunPlan &p, cudaStream_t st,
                           bcg_stats *stats) {
-    // the labelling job's outcome is kept: a failed job fails this run and
-    // every later one (its labels are incomplete)
-    if (g->comp_job.valid()) g->comp_rc = g->comp_job.get();
-    if (g->comp_rc != BCG_OK) return set_error(BCG_ERR_OOM, "labelling the components: out of host memory");
-    std::vector<uint32_t> cnt(g->n, 0);
+    std::vector<uint32_t> s;
+    s.reserve(nsrc);
     for (uint64_t i = 0; i < nsrc; ++i)
-        if (g->h_deg[src[i]]) ++cnt[src[i]];
-    std::vector<double> acc;
-    tree_bc(g->tinfo, cnt, acc);
-    CK(cudaMemcpyAsync(g->d_tree_acc, acc.data(), (size_t)g->n * sizeof(double), cudaMemcpyHostToDevice, st));
-    k_add<<<(g->n + 255) / 256, 256, 0, st>>>(g->n, g->d_bc, g->d_tree_acc);
-    CK(cudaGetLastError());
-    CK(cudaStreamSynchronize(st));
+        if (g->h_deg[src[i]]) s.push_back(src[i]);
+    const int rc = tree_terms(g, s, st);
+    if (rc) return rc;
     if (stats) {
         stats->teps_edges += p.tree_edges;
         stats->comp_vertices += p.tree_verts;
@@ -403,8 +391,8 @@ static int plan_run(const bcg_graph *g, const uint32_t *src, uint64_t nsrc, RunP
             // a tree component: no kept edges, its bc is all in the tree terms
             // (the kept vertex r is the last one of its tree: sz[r] is the component)
             ++p.tree_only;
-            p.tree_edges += g->tinfo.sz[r] - 1;
-            p.tree_verts += g->tinfo.sz[r];
+            p.tree_edges += g->h_sz[r] - 1;
+            p.tree_verts += g->h_sz[r];
             continue;
         }
         auto it = idx.find(r);
@@ -681,34 +669,14 @@ static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint3
         rc = validate_csr(offsets, adj, n, nnz);
         if (rc) return rc;
     }
-    // iterated pendant-tree pruning: the device holds the kept graph only
+    // iterated pendant-tree pruning: the device peels the trees and keeps
+    // the kept graph only
     const bool trees = (flags & BCG_PRUNE_TREES) && !(flags & BCG_DIRECTED);
-    bcg::TreeInfo tinfo;
-    std::vector<uint32_t> cdeg, h_adj_copy, ext, intl, lab_offs, lab_adj;
-    uint32_t nlive = 0;
-    const uint32_t *orig_offs = ho;
-    if (trees) {
-        const uint32_t *hadj = adj;
-        if (device_in) {
-            h_adj_copy.resize(nnz);
-            if (nnz && cudaMemcpy(h_adj_copy.data(), adj, nnz * sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
-                return set_error(BCG_ERR_CUDA, "reading adjacency");
-            for (uint64_t e = 0; e < nnz; ++e)
-                if (h_adj_copy[e] >= n) return set_error(BCG_ERR_ARG, "adj[%" PRIu64 "] = %u >= n", e, h_adj_copy[e]);
-            hadj = h_adj_copy.data();
-        }
-        nlive = peel_trees(ho, hadj, n, tinfo, cdeg, ext, intl, lab_offs, lab_adj);
-        offsets = lab_offs.data();
-        adj = lab_adj.data();
-        ho = lab_offs.data();
-        device_in = false;
-        flags &= ~BCG_PRUNE_DEGREE1;
-    }
-    const uint64_t dev_nnz = trees ? lab_adj.size() : nnz;
+    if (trees) flags &= ~BCG_PRUNE_DEGREE1;
     bcg_graph *g = new bcg_graph();
     cudaGetDevice(&g->device);
     g->n = n;
-    g->nnz = dev_nnz;
+    g->nnz = nnz;
     g->flags = flags;
     if (const char *e = getenv("BCG_PUSH_PULL_RATIO")) g->ratio = (float)atof(e);
     if (const char *e = getenv("BCG_TILE_SHAPE")) {  // "<vertices>x<entries>", e.g. 32x128
@@ -719,61 +687,58 @@ static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint3
             g->tile_ecap = te;
         }
     }
-    if (trees) g->tile_n = nlive ? nlive : 1;
     auto fail = [&](int code) { graph_free(g); return code; };
     cudaError_t e;
-    // 4 entries of tail padding on offsets and adjacency: the sweep copies
-    // their ranges in 16-byte aligned pieces that may end up to 12 bytes
-    // past the last entry
-    if ((e = cudaMalloc(&g->d_offs, ((size_t)n + 1 + 4) * sizeof(uint32_t))) != cudaSuccess ||
-        (e = cudaMalloc(&g->d_adj, (dev_nnz + 4) * sizeof(uint32_t))) != cudaSuccess)
-        return fail(set_error(BCG_ERR_OOM, "cudaMalloc CSR: %s", cudaGetErrorString(e)));
-    const cudaMemcpyKind kind = device_in ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    if ((e = cudaMemcpy(g->d_offs, offsets, ((size_t)n + 1) * sizeof(uint32_t), kind)) != cudaSuccess ||
-        (e = cudaMemset(g->d_offs + n + 1, 0, 4 * sizeof(uint32_t))) != cudaSuccess ||
-        (dev_nnz && (e = cudaMemcpy(g->d_adj, adj, dev_nnz * sizeof(uint32_t), kind)) != cudaSuccess) ||
-        (e = cudaMemset(g->d_adj + dev_nnz, 0, 4 * sizeof(uint32_t))) != cudaSuccess)
-        return fail(set_error(BCG_ERR_CUDA, "uploading CSR: %s", cudaGetErrorString(e)));
-    rc = create_common(g, ho);
+    std::vector<uint32_t> h_offs2;
+    if (trees) {
+        // the input CSR on the device (a temporary copy for host input)
+        const uint32_t *d_offs0 = offsets, *d_adj0 = adj;
+        uint32_t *t_offs = nullptr, *t_adj = nullptr;
+        auto drop = [&]() { cudaFree(t_offs); cudaFree(t_adj); };
+        if (!device_in) {
+            if ((e = cudaMalloc(&t_offs, ((size_t)n + 1) * sizeof(uint32_t))) != cudaSuccess ||
+                (e = cudaMalloc(&t_adj, std::max<uint64_t>(nnz, 1) * sizeof(uint32_t))) != cudaSuccess ||
+                (e = cudaMemcpy(t_offs, offsets, ((size_t)n + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice)) !=
+                    cudaSuccess ||
+                (nnz && (e = cudaMemcpy(t_adj, adj, nnz * sizeof(uint32_t), cudaMemcpyHostToDevice)) != cudaSuccess)) {
+                drop();
+                return fail(set_error(e == cudaErrorMemoryAllocation ? BCG_ERR_OOM : BCG_ERR_CUDA,
+                                      "uploading CSR: %s", cudaGetErrorString(e)));
+            }
+            d_offs0 = t_offs;
+            d_adj0 = t_adj;
+        }
+        rc = prepare_trees(g, d_offs0, d_adj0, nnz, device_in, h_offs2);
+        drop();
+        if (rc) return fail(rc);
+        g->nnz = h_offs2[n];  // kept entries, while the common setup runs
+    } else {
+        // 4 entries of tail padding on offsets and adjacency: the sweep copies
+        // their ranges in 16-byte aligned pieces that may end up to 12 bytes
+        // past the last entry
+        if ((e = cudaMalloc(&g->d_offs, ((size_t)n + 1 + 4) * sizeof(uint32_t))) != cudaSuccess ||
+            (e = cudaMalloc(&g->d_adj, (nnz + 4) * sizeof(uint32_t))) != cudaSuccess)
+            return fail(set_error(BCG_ERR_OOM, "cudaMalloc CSR: %s", cudaGetErrorString(e)));
+        const cudaMemcpyKind kind = device_in ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        if ((e = cudaMemcpy(g->d_offs, offsets, ((size_t)n + 1) * sizeof(uint32_t), kind)) != cudaSuccess ||
+            (e = cudaMemset(g->d_offs + n + 1, 0, 4 * sizeof(uint32_t))) != cudaSuccess ||
+            (nnz && (e = cudaMemcpy(g->d_adj, adj, nnz * sizeof(uint32_t), kind)) != cudaSuccess) ||
+            (e = cudaMemset(g->d_adj + nnz, 0, 4 * sizeof(uint32_t))) != cudaSuccess)
+            return fail(set_error(BCG_ERR_CUDA, "uploading CSR: %s", cudaGetErrorString(e)));
+    }
+    rc = create_common(g, trees ? h_offs2.data() : ho);
     if (rc) return fail(rc);
     if (trees) {
-        // kept-graph degrees for the searches, input degrees for the source
-        // skip test, and every kept vertex weighted by its trees (reach)
+        // kept-graph degrees and tree weights (reach) for the searches, input
+        // degrees for the source skip test
         g->trees = true;
         g->nnz = nnz;
-        g->h_cdeg = std::move(cdeg);
-        for (uint32_t v = 0; v < n; ++v) g->h_deg[v] = orig_offs[v + 1] - orig_offs[v];
-        g->tinfo = std::move(tinfo);
-        g->h_anchor = g->tinfo.anchor;
-        g->npruned = (uint32_t)g->tinfo.order.size();
-        std::vector<uint2> vi(n);  // internal numbering
-        for (uint32_t i = 0; i < n; ++i) {
-            const uint32_t v = ext[i];
-            vi[i] = make_uint2(g->h_cdeg[v], g->tinfo.parent[v] == kNoRoot ? g->tinfo.sz[v] - 1 : 0u);
-        }
-        if ((e = cudaMemcpy(g->d_vinfo, vi.data(), (size_t)n * sizeof(uint2), cudaMemcpyHostToDevice)) != cudaSuccess ||
-            (e = cudaMalloc(&g->d_tree_acc, (size_t)n * sizeof(double))) != cudaSuccess ||
-            (e = cudaMalloc(&g->d_ext, (size_t)n * sizeof(uint32_t))) != cudaSuccess ||
-            (e = cudaMemcpy(g->d_ext, ext.data(), (size_t)n * sizeof(uint32_t), cudaMemcpyHostToDevice)) != cudaSuccess)
+        for (uint32_t v = 0; v < n; ++v) g->h_deg[v] = ho[v + 1] - ho[v];
+        if ((e = cudaMemcpy(g->d_vinfo, g->d_vinfo_trees, (size_t)n * sizeof(uint2), cudaMemcpyDeviceToDevice)) !=
+            cudaSuccess)
             return fail(set_error(BCG_ERR_CUDA, "tree weights: %s", cudaGetErrorString(e)));
-        g->h_intl = std::move(intl);
-        g->h_lab_offs = std::move(lab_offs);
-        g->h_lab_adj = std::move(lab_adj);
-        auto job = [g]() {
-            try {
-                label_components(g->h_lab_offs.data(), g->h_lab_adj.data(), g->n, g->h_intl, g->tinfo);
-            } catch (...) {
-                return (int)BCG_ERR_OOM;
-            }
-            std::vector<uint32_t>().swap(g->h_lab_offs);
-            std::vector<uint32_t>().swap(g->h_lab_adj);
-            return (int)BCG_OK;
-        };
-        try {
-            g->comp_job = std::async(std::launch::async, job);
-        } catch (...) {  // no thread to be had: label them now
-            if (job() != BCG_OK) return fail(set_error(BCG_ERR_OOM, "labelling the components: out of host memory"));
-        }
+        cudaFree(g->d_vinfo_trees);
+        g->d_vinfo_trees = nullptr;
     }
     *out = g;
     return BCG_OK;

@@ -2,7 +2,6 @@
 // translation units (engine.cu: single graphs; batch.cu: packed unions of
 // graphs).  Not part of the public ABI.
 #pragma once
-#include <future>
 #include <vector>
 
 #include "bcg.h"
@@ -17,14 +16,20 @@ using bcg::kTileEdges;
 using bcg::kTileVerts;
 
 namespace bcg {
-// Pendant trees of a graph (BCG_PRUNE_TREES; trees.cpp).
-struct TreeInfo {
-    std::vector<uint32_t> parent;  // vertex it hung from when peeled; kNoRoot for kept (core) vertices
-    std::vector<uint32_t> order;   // peeled vertices, in peeling order (children before parents)
-    std::vector<uint32_t> sz;      // vertices in the subtree (a kept vertex: 1 + its trees)
-    std::vector<uint32_t> anchor;  // the kept vertex a vertex's tree hangs from (itself if kept)
-    std::vector<uint32_t> comp;    // connected component of the input graph
-    std::vector<uint64_t> comp_n;  // vertices per component
+// Pendant trees of a graph on the device (BCG_PRUNE_TREES; trees_gpu.cu),
+// caller's numbering.
+struct TreeDev {
+    uint32_t *parent = nullptr;  // vertex it hung from when peeled; kNoRoot for kept vertices
+    uint32_t *sz = nullptr;      // vertices in the subtree (a kept vertex: 1 + its trees)
+    uint32_t *comp = nullptr;    // component of the input graph (a root's internal id)
+    unsigned long long *comp_n = nullptr;  // vertices per component, indexed by root
+    uint32_t *order = nullptr;   // peeled vertices, round by round
+    std::vector<uint32_t> round_off;  // start of each round in order, and the end
+    uint32_t npeeled = 0;
+    // per-run scratch of the closed-form tree terms
+    uint32_t *cnt = nullptr, *src = nullptr;
+    size_t src_cap = 0;
+    unsigned long long *sub = nullptr, *csrc = nullptr, *acc = nullptr;
 };
 }  // namespace bcg
 
@@ -59,9 +64,11 @@ struct bcg_graph {
     uint32_t tile_vcap = kTileVerts, tile_ecap = kTileEdges;  // tile shape (autotuned by batches)
     std::vector<uint32_t> tile_breaks;  // sorted vertices where a new tile must start
     float ratio = 0.2f;
-    bool trees = false;               // BCG_PRUNE_TREES: pendant trees folded (tinfo)
-    bcg::TreeInfo tinfo;
+    bool trees = false;               // BCG_PRUNE_TREES: pendant trees folded (tdev)
+    bcg::TreeDev tdev;
     std::vector<uint32_t> h_cdeg;     // degrees in the kept graph, caller's numbering (trees mode)
+    std::vector<uint32_t> h_sz;       // subtree sizes, caller's numbering (trees mode)
+    uint2 *d_vinfo_trees = nullptr;   // degree/reach words built by the peeling (until creation ends)
     // Trees mode numbers the searched vertices internally: the vertices with
     // kept edges first (caller's order), then the rest, so the tiles cover
     // [0, tile_n) only.  h_intl: caller's id -> internal id; d_ext: internal
@@ -69,13 +76,6 @@ struct bcg_graph {
     uint32_t tile_n = 0;              // vertices covered by tiles (0: all n)
     std::vector<uint32_t> h_intl;     // empty: internal ids are the caller's
     uint32_t *d_ext = nullptr;
-    // trees mode: the components are labelled on a host thread that overlaps
-    // the first run's searches (from a copy of the kept graph's CSR); the
-    // closed-form tree terms wait for it
-    std::vector<uint32_t> h_lab_offs, h_lab_adj;
-    std::future<int> comp_job;
-    int comp_rc = BCG_OK;             // the job's result once taken from the future
-    double *d_tree_acc = nullptr;     // tree vertices' closed-form bc of one run
     int sigma_mode = 0;               // 0 auto (exact, extended on overflow), 1 exact only, 2 extended
     double *d_bc_save = nullptr;      // accumulators before an automatic-mode run
     unsigned long long wait_ns = kDefaultWaitNs;
@@ -108,22 +108,18 @@ int enqueue_packed(bcg_graph *g, const PackedRun &p, uint32_t S, cudaStream_t st
 int check_ctrl(bcg_graph *g, cudaStream_t st);
 // Rebuilds the work tiles with another shape (vcap vertices, ecap entries).
 int graph_retile(bcg_graph *g, uint32_t vcap, uint32_t ecap, bool force = false);
-// Peels every pendant tree off the graph (t: all but the components) and
-// returns the kept graph renumbered so the vertices that keep an edge come
-// first (in their order), then the rest: ext[i] = id of internal vertex i,
-// intl its inverse, (offs2, adj2) the renumbered CSR, cdeg[v] = v's degree
-// in the kept graph.  Returns the number of vertices that keep an edge.
-uint32_t peel_trees(const uint32_t *offs, const uint32_t *adj, uint32_t n, TreeInfo &t, std::vector<uint32_t> &cdeg,
-                    std::vector<uint32_t> &ext, std::vector<uint32_t> &intl, std::vector<uint32_t> &offs2,
-                    std::vector<uint32_t> &adj2);
-// Labels the components of every vertex (t.comp, t.comp_n) from the kept
-// graph's CSR (internal ids; intl: id -> internal id, empty: the same) and
-// the anchors.
-void label_components(const uint32_t *offs, const uint32_t *adj, uint32_t n, const std::vector<uint32_t> &intl,
-                      TreeInfo &t);
-// Closed-form bc of the tree vertices (and the anchors' tree terms) for the
-// source multiplicities cnt[v].
-void tree_bc(const TreeInfo &t, const std::vector<uint32_t> &cnt, std::vector<double> &acc);
+// Peels the pendant trees of the input CSR (device arrays d_offs0 / d_adj0,
+// nnz entries; check_ids: verify every id < n first) and builds g's kept
+// graph in internal numbering (d_offs, d_adj, d_ext, tile_n, degree/reach
+// words in d_vinfo_trees), the tree arrays (tdev) and the host lookups
+// (h_anchor, h_cdeg, h_intl, h_sz).  h_offs2: the kept graph's offsets.
+int prepare_trees(bcg_graph *g, const uint32_t *d_offs0, const uint32_t *d_adj0, uint64_t nnz, bool check_ids,
+                  std::vector<uint32_t> &h_offs2);
+// Adds the closed-form betweenness of the tree vertices (and the anchors'
+// tree terms) for the sources src (degree > 0, caller's ids, duplicates
+// count) into g's bc, on stream st.
+int tree_terms(bcg_graph *g, const std::vector<uint32_t> &src, cudaStream_t st);
+void tree_free(bcg_graph *g);
 // Uploads ngraphs host CSR graphs as one disjoint union (graph order[p] at
 // union position p, its vertex v at base[order[p]] + v; with by_active the
 // graphs with most non-isolated vertices come first).  hdeg: union degrees.

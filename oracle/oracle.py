@@ -135,5 +135,30 @@ def bc_q(offsets, adj, sources, nthreads: int = 1):
     return out, {f: getattr(st, f) for f, _ in st._fields_}
 
 
+_TREES = None
+
+
+def peel_trees(offsets, adj):
+    """Host restatement of pendant-tree peeling (trees_ref.cpp) ->
+    (anchor uint32[n], subtree size uint32[n], peeled vertex count)."""
+    global _TREES
+    if _TREES is None:
+        path = os.path.join(HERE, "libtrees_ref.so")
+        if not os.path.exists(path):
+            subprocess.run(["make", "-s", "-C", HERE, "libtrees_ref.so"], check=True)
+        L = ctypes.CDLL(path)
+        L.oracle_peel_trees.restype = ctypes.c_int
+        L.oracle_peel_trees.argtypes = [ctypes.c_uint32, _u32p, _u32p, _u32p, _u32p, _u64p]
+        _TREES = L
+    offsets, adj = _u32(offsets), _u32(adj)
+    n = len(offsets) - 1
+    anc = np.zeros(n, np.uint32)
+    sz = np.zeros(n, np.uint32)
+    npl = ctypes.c_uint64(0)
+    _TREES.oracle_peel_trees(n, offsets.ctypes.data_as(_u32p), adj.ctypes.data_as(_u32p), anc.ctypes.data_as(_u32p),
+                             sz.ctypes.data_as(_u32p), ctypes.byref(npl))
+    return anc, sz, int(npl.value)
+
+
 def max_threads() -> int:
     return lib().oracle_max_threads()

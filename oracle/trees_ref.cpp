@@ -1,15 +1,18 @@
-// Iterative pendant-tree pruning (BCG_PRUNE_TREES): the reference folds one
-// layer of degree-1 vertices (degree_reduction, bc2d.c:314-419); here whole
-// trees hanging off the graph's 2-core are folded and their betweenness is
-// computed in closed form.
+// ORACLE — test infrastructure only (never linked into the product).
 //
-// Peeling removes degree-1 vertices until none is left; every removed vertex v
-// records the neighbour it hung from (parent[v]), so the removed vertices form
-// trees rooted at the remaining ("core") vertices, their anchors.  A component
-// that is a tree keeps one vertex, the last one peeled to degree 0.
+// Host restatement of iterated pendant-tree pruning and of the closed-form
+// betweenness of the tree vertices, which the engine computes on the device
+// (ck-bc_b200/csrc/trees_gpu.cu).  tests/test_trees.py pins the closed form
+// against the Brandes oracle on forests, and tests/test_gpu_trees.py checks
+// the device peeling's kept set and subtree weights against this one.  The
+// reference folds one layer of degree-1 vertices (degree_reduction,
+// bc2d.c:314-419); this restatement folds whole trees.
 //
-// Components: a tree vertex's component is its anchor's, so the components
-// are labelled on the kept graph alone (label_components).
+// Peeling removes degree-1 vertices until none is left (a FIFO queue); every
+// removed vertex v records the neighbour it hung from (parent[v]), so the
+// removed vertices form trees rooted at the remaining ("core") vertices, their
+// anchors.  A component that is a tree keeps one vertex, the last one peeled
+// to degree 0.
 //
 // Exactness (ordered pairs (s, t), s a requested source):
 //   - A path between two vertices of one tree, or between a tree vertex and
@@ -18,22 +21,15 @@
 //     (s, t) exactly when s and t sit in different branches at v (its child
 //     subtrees and "the rest of the component"), and
 //       bc[v] += sum over branches B at v of (sources in B) * (n_comp - 1 - |B|).
-//   - An anchor a gets the same terms for its child subtrees; pairs with the
-//     source outside its tree are counted by the core search below.
-//   - The core is searched from every anchor a that is requested or holds
-//     requested sources in its tree, with weight mult(a) = [a in S] +
-//     (sources in T_a), and every core vertex weighs 1 + reach (its tree's
-//     size - 1) as a target (the engine's reach weights, init_delta
-//     cuda_kernels.cu:1089-1098).  Tree sources have no other core term: their
-//     paths through a are in the tree terms above.
+//   - An anchor a gets the same terms for its child subtrees.
 #include <algorithm>
 #include <cstdint>
 #include <deque>
 #include <vector>
 
-#include "engine_internal.hpp"
+#include "trees_ref.hpp"
 
-namespace bcg {
+namespace oracle_trees {
 
 uint32_t peel_trees(const uint32_t *offs, const uint32_t *adj, uint32_t n, TreeInfo &t, std::vector<uint32_t> &cdeg,
                     std::vector<uint32_t> &ext, std::vector<uint32_t> &intl, std::vector<uint32_t> &offs2,
@@ -176,4 +172,19 @@ void tree_bc(const TreeInfo &t, const std::vector<uint32_t> &cnt, std::vector<do
     }
 }
 
-}  // namespace bcg
+}  // namespace oracle_trees
+
+// C entry for the Python wrapper: anchors and subtree sizes of every vertex
+// after peeling, and the number of peeled vertices.
+extern "C" int oracle_peel_trees(uint32_t n, const uint32_t *offs, const uint32_t *adj, uint32_t *anchor,
+                                 uint32_t *sz, uint64_t *npeeled) {
+    oracle_trees::TreeInfo t;
+    std::vector<uint32_t> cdeg, ext, intl, o2, a2;
+    oracle_trees::peel_trees(offs, adj, n, t, cdeg, ext, intl, o2, a2);
+    for (uint32_t v = 0; v < n; ++v) {
+        anchor[v] = t.anchor[v];
+        sz[v] = t.sz[v];
+    }
+    *npeeled = t.order.size();
+    return 0;
+}

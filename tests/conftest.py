@@ -19,8 +19,9 @@ def pytest_configure(config):
 def _ensure_built():
     if not os.path.exists(os.path.join(PKG, "libbcg.so")) or not os.path.exists(os.path.join(PKG, "bc2d")):
         subprocess.run(["make", "-s", "-C", PKG], check=True)
-    if not os.path.exists(os.path.join(ORACLE, "liboracle.so")):
-        subprocess.run(["make", "-s", "-C", ORACLE, "liboracle.so"], check=True)
+    for lib in ("liboracle.so", "libtrees_ref.so"):
+        if not os.path.exists(os.path.join(ORACLE, lib)):
+            subprocess.run(["make", "-s", "-C", ORACLE, lib], check=True)
 
 
 _ensure_built()

@@ -63,3 +63,32 @@ def test_tree_component_and_refusals():
         reach = np.zeros(9, dtype=np.uint32)
         with pytest.raises(bcg.BcgError):
             bcg._check(bcg.lib().bcg_graph_set_reach(G.h, bcg._p32(reach)))
+
+
+@pytest.mark.parametrize("spec", list(SPECS.values()) +
+                         ["rmat:scale=20,ef=16,a=0.57,b=0.19,c=0.19,seed=2,pendant_frac=0.1,pendant_mean=4"])
+def test_device_peeling_matches_host(spec):
+    """The device peeling against the oracle's host restatement: the same
+    number of peeled vertices, the same anchor for every vertex of a component
+    that keeps a cycle (its 2-core is unique), and in every tree component
+    exactly one kept vertex that all its vertices hang from."""
+    from scipy.sparse import csr_matrix
+    from scipy.sparse.csgraph import connected_components
+
+    offs, adj = bcg.generate(spec)
+    n = len(offs) - 1
+    anc_h, _, np_h = oracle.peel_trees(offs, adj)
+    with bcg.Graph(offs, adj, bcg.PRUNE_TREES) as G:
+        anc_d, _ = G.pruning()
+        np_d = G.info()["pruned"]
+    assert np_d == np_h
+    ncomp, lab = connected_components(csr_matrix((np.ones(len(adj)), adj, offs), shape=(n, n)), directed=False)
+    vcount = np.bincount(lab, minlength=ncomp)
+    ecount = np.bincount(lab, weights=np.diff(offs), minlength=ncomp) / 2
+    tree_comp = ecount == vcount - 1
+    in_tree = tree_comp[lab]
+    assert np.array_equal(anc_d[~in_tree], anc_h[~in_tree])
+    ids = np.arange(n, dtype=np.uint32)
+    kept_d = anc_d == ids
+    assert np.array_equal(np.bincount(lab[kept_d & in_tree], minlength=ncomp)[tree_comp], np.ones(tree_comp.sum()))
+    assert np.all(lab[anc_d] == lab)

@@ -1,6 +1,6 @@
-"""Iterated pendant-tree pruning, host part (CPU only).
+"""Iterated pendant-tree pruning: the oracle's host restatement (CPU only).
 
-ck-bc_b200/csrc/trees.cpp is compiled into a small harness.  On a forest
+oracle/trees_ref.cpp is compiled into a small harness.  On a forest
 every vertex is peeled (or is the last vertex of its tree), no core search
 runs, and the closed-form tree terms must equal the oracle's Brandes bc for
 any source multiset."""
@@ -18,8 +18,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HARNESS = r"""
 #include <cstdio>
 #include <vector>
-#include "engine_internal.hpp"
-using namespace bcg;
+#include "trees_ref.hpp"
+using namespace oracle_trees;
 int main() {
     unsigned n, m, k;
     if (scanf("%u %u %u", &n, &m, &k) != 3) return 1;
@@ -44,9 +44,9 @@ def harness(tmp_path_factory):
     d = tmp_path_factory.mktemp("trees")
     (d / "h.cpp").write_text(HARNESS)
     exe = d / "h"
-    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "ck-bc_b200", "csrc"), "-I",
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "oracle"), "-I",
                     os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include",
-                    os.path.join(ROOT, "ck-bc_b200", "csrc", "trees.cpp"), str(d / "h.cpp"), "-o", str(exe)],
+                    os.path.join(ROOT, "oracle", "trees_ref.cpp"), str(d / "h.cpp"), "-o", str(exe)],
                    check=True)
 
     def run(offs, adj, src):
@@ -94,8 +94,8 @@ def test_peeling_anchors_and_core(harness):
 RELABEL = r"""
 #include <cstdio>
 #include <vector>
-#include "engine_internal.hpp"
-using namespace bcg;
+#include "trees_ref.hpp"
+using namespace oracle_trees;
 int main() {
     unsigned n, m;
     if (scanf("%u %u", &n, &m) != 2) return 1;
@@ -121,9 +121,9 @@ def test_relabel_keeps_the_kept_graph(tmp_path):
     order; the renumbered CSR is that graph."""
     (tmp_path / "r.cpp").write_text(RELABEL)
     exe = tmp_path / "r"
-    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "ck-bc_b200", "csrc"), "-I",
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "oracle"), "-I",
                     os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include",
-                    os.path.join(ROOT, "ck-bc_b200", "csrc", "trees.cpp"), str(tmp_path / "r.cpp"), "-o", str(exe)],
+                    os.path.join(ROOT, "oracle", "trees_ref.cpp"), str(tmp_path / "r.cpp"), "-o", str(exe)],
                    check=True)
     offs, adj = bcg.generate("rmat:scale=9,ef=4,seed=5,pendant_frac=0.3,pendant_mean=5")
     n = len(offs) - 1
@@ -147,8 +147,8 @@ def test_relabel_keeps_the_kept_graph(tmp_path):
 COMPONENTS = r"""
 #include <cstdio>
 #include <vector>
-#include "engine_internal.hpp"
-using namespace bcg;
+#include "trees_ref.hpp"
+using namespace oracle_trees;
 int main() {
     unsigned n, m;
     if (scanf("%u %u", &n, &m) != 2) return 1;
@@ -176,9 +176,9 @@ def test_parallel_components_match_scipy(tmp_path, spec):
     import scipy.sparse as sp
     (tmp_path / "c.cpp").write_text(COMPONENTS)
     exe = tmp_path / "c"
-    subprocess.run(["g++", "-O2", "-std=c++17", "-fopenmp", "-I", os.path.join(ROOT, "ck-bc_b200", "csrc"), "-I",
+    subprocess.run(["g++", "-O2", "-std=c++17", "-fopenmp", "-I", os.path.join(ROOT, "oracle"), "-I",
                     os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include",
-                    os.path.join(ROOT, "ck-bc_b200", "csrc", "trees.cpp"), str(tmp_path / "c.cpp"), "-o", str(exe)],
+                    os.path.join(ROOT, "oracle", "trees_ref.cpp"), str(tmp_path / "c.cpp"), "-o", str(exe)],
                    check=True)
     offs, adj = bcg.generate(spec)
     n = len(offs) - 1
