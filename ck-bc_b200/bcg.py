@@ -106,6 +106,8 @@ SIGNATURES = {
     "bcg_graph_set_reach": (ctypes.c_int, [ctypes.c_void_p, _u32p]),
     "bcg_run_weighted": (ctypes.c_int, [ctypes.c_void_p, _u32p, _f64p, _u32p, ctypes.c_uint64,
                                         ctypes.POINTER(Stats)]),
+    "bcg_run_root_levels": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_double, ctypes.c_uint32,
+                                           _i32p, ctypes.POINTER(Stats)]),
     "bcg_set_batch_width": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32]),
     "bcg_set_sigma_mode": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "bcg_single_source_ext": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, _i32p, _u64p, _f64p]),

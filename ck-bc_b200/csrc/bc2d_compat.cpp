@@ -24,6 +24,8 @@ std::vector<int32_t> g_level;      // BFS depth of the current source (-1 = not 
 std::vector<uint32_t> g_count;     // vertices per level of the current source
 uint32_t g_v0 = 0;
 uint32_t g_reach_v0 = 0;
+bool g_pending = false;            // the current source's search has not run yet
+uint64_t g_reach_visited = 0;      // sum of reach over the vertices it reached, root excluded
 
 [[noreturn]] void fail(const char *what, int rc) {
     fprintf(stderr, "bc2d_compat: %s failed (%d): %s\n", what, rc, bcg_last_error());
@@ -57,37 +59,49 @@ void setcuda(uint64_t, LOCINT *, LOCINT *, LOCINT reach_v0) {
     g_count.clear();
 }
 
+// The driver's per-source sequence (bc_func_mono, bc2d.c:504-580) is
+// setcuda, set_mlp_cuda, then scan_col_csc_cuda_mono per level inside its
+// timer, the scan_frt_csc_cuda_mono calls, pre_update_bc_cuda and
+// update_bc_cuda.  The engine does the whole source in one search: the first
+// level call runs it (weighted by the root's folded pendants, exporting the
+// depths), the later calls return the per-level counts it found, and
+// update_bc_cuda has nothing left to do.
 void set_mlp_cuda(LOCINT row, int, int) {
     g_v0 = row;
-    int rc = bcg_single_source(g_graph, row, g_level.data(), nullptr, nullptr);
-    if (rc) fail("set_mlp_cuda", rc);
+    g_pending = true;
+    g_count.clear();
+}
+
+static void run_source() {
+    const double mult = (double)g_reach_v0 + 1.0;
+    bcg_stats st{};
+    int rc = bcg_run_root_levels(g_graph, g_v0, mult, g_reach_v0, g_level.data(), &st);
+    if (rc) fail("scan_col_csc_cuda_mono", rc);
+    g_pending = false;
     g_count.clear();
     for (int32_t l : g_level) {
         if (l < 0) continue;
         if ((size_t)l >= g_count.size()) g_count.resize(l + 1, 0);
         ++g_count[l];
     }
+    // comp_vertices = sum of (1 + reach) over the reached vertices
+    g_reach_visited = st.comp_vertices - st.visited - g_reach_v0;
 }
 
 LOCINT scan_col_csc_cuda_mono(int, int level) {
+    if (g_pending) run_source();
     return (level >= 0 && (size_t)level < g_count.size()) ? g_count[level] : 0u;
 }
 
 LOCINT scan_frt_csc_cuda_mono(int, int ncol, int) { return (LOCINT)ncol; }
 
-void pre_update_bc_cuda(LOCINT *reach, uint64_t, LOCINT *all) {
-    uint64_t s = 0;
-    for (size_t v = 0; v < g_level.size(); ++v)
-        if (g_level[v] > 0) s += reach[v];
-    *all = (LOCINT)s;
+void pre_update_bc_cuda(LOCINT *, uint64_t, LOCINT *all) {
+    if (g_pending) run_source();
+    *all = (LOCINT)g_reach_visited;
 }
 
-void update_bc_cuda(uint64_t v0, int, const uint64_t) {
-    const uint32_t root = (uint32_t)v0;
-    const double mult = (double)g_reach_v0 + 1.0;
-    const uint32_t pend = g_reach_v0;
-    int rc = bcg_run_weighted(g_graph, &root, &mult, &pend, 1, nullptr);
-    if (rc) fail("update_bc_cuda", rc);
+void update_bc_cuda(uint64_t, int, const uint64_t) {
+    if (g_pending) run_source();  // a driver that skipped the level calls
 }
 
 void get_msk(LOCINT *msk) {

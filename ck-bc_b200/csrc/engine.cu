@@ -190,6 +190,7 @@ static void graph_free(bcg_graph *g) {
     cudaFree(g->d_lbase); cudaFree(g->d_lcnt); cudaFree(g->d_ulist); cudaFree(g->d_bc_save);
     tree_free(g);
     cudaFree(g->d_vinfo_trees);
+    cudaFree(g->d_level_out);
     cudaFree(g->d_ext);
     cudaFree(g->d_rows); cudaFree(g->d_ctrl);
     cudaFree(g->d_roots); cudaFree(g->d_pend); cudaFree(g->d_mult); cudaFree(g->d_rstat);
@@ -738,6 +739,7 @@ static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint3
             cudaSuccess)
             return fail(set_error(BCG_ERR_CUDA, "tree weights: %s", cudaGetErrorString(e)));
         cudaFree(g->d_vinfo_trees);
+    cudaFree(g->d_level_out);
         g->d_vinfo_trees = nullptr;
     }
     *out = g;
@@ -1006,6 +1008,31 @@ int bcg_run_weighted(bcg_graph *g, const uint32_t *roots, const double *mult, co
         p.count.push_back(1);
     }
     return run_plan(g, p, 0, st, DebugOut{});
+}
+
+int bcg_run_root_levels(bcg_graph *g, uint32_t root, double mult, uint32_t pend, int32_t *level,
+                        bcg_stats *stats) {
+    clear_error();
+    if (!g || !level) return set_error(BCG_ERR_ARG, "null argument");
+    if (g->trees) return set_error(BCG_ERR_ARG, "graph was created with BCG_PRUNE_TREES");
+    if (root >= g->n) return set_error(BCG_ERR_ARG, "root %u >= n=%u", root, g->n);
+    bcg_stats local{};
+    bcg_stats *st = stats ? stats : &local;
+    *st = bcg_stats{};
+    st->sources = 1;
+    RunPlan p;
+    p.roots.push_back(root);
+    p.mult.push_back(mult);
+    p.pend.push_back(pend);
+    p.count.push_back(1);
+    if (!g->d_level_out) CK(cudaMalloc(&g->d_level_out, (size_t)g->n * sizeof(int32_t)));
+    DebugOut out;  // width 1, levels only: bc accumulates as in a plain run
+    out.width = 1;
+    out.level = g->d_level_out;
+    int rc = run_plan(g, p, 0, st, out);
+    if (rc) return rc;
+    CK(cudaMemcpy(level, g->d_level_out, (size_t)g->n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    return BCG_OK;
 }
 
 int bcg_set_batch_width(bcg_graph *g, uint32_t width) {

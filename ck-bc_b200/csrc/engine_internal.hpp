@@ -69,6 +69,7 @@ struct bcg_graph {
     std::vector<uint32_t> h_cdeg;     // degrees in the kept graph, caller's numbering (trees mode)
     std::vector<uint32_t> h_sz;       // subtree sizes, caller's numbering (trees mode)
     uint2 *d_vinfo_trees = nullptr;   // degree/reach words built by the peeling (until creation ends)
+    int32_t *d_level_out = nullptr;   // depths exported by bcg_run_root_levels
     // Trees mode numbers the searched vertices internally: the vertices with
     // kept edges first (caller's order), then the rest, so the tiles cover
     // [0, tile_n) only.  h_intl: caller's id -> internal id; d_ext: internal

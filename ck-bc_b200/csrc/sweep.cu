@@ -1222,17 +1222,17 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
         }
         const uint32_t D = d;
 
-        if (a.dbg_sigma) {
-            // debug run: copy every slot's levels and sigma out before the
-            // backward pass overwrites sigma
+        if (a.dbg_level || a.dbg_sigma) {
+            // debug or level-export run: copy every slot's levels (and sigma)
+            // out before the backward pass overwrites sigma
             for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < a.n;
                  v += (size_t)gridDim.x * blockDim.x) {
                 unsigned char *row = a.rows + v * R;
 #pragma unroll
                 for (int k = 0; k < S; ++k) {
                     const uint16_t L = *lvl_at(row, k);
-                    a.dbg_level[(size_t)k * a.n + v] = (L == kUnvisited) ? -1 : (int32_t)L;
-                    a.dbg_sigma[(size_t)k * a.n + v] = (L == kUnvisited) ? 0ull : *val_at<S>(row, k);
+                    if (a.dbg_level) a.dbg_level[(size_t)k * a.n + v] = (L == kUnvisited) ? -1 : (int32_t)L;
+                    if (a.dbg_sigma) a.dbg_sigma[(size_t)k * a.n + v] = (L == kUnvisited) ? 0ull : *val_at<S>(row, k);
                 }
             }
             if (!grid_sync(c, nblk, wait_ns)) return;

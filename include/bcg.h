@@ -230,6 +230,14 @@ int bcg_graph_set_reach(bcg_graph *g, const uint32_t *reach);
 int bcg_run_weighted(bcg_graph *g, const uint32_t *roots, const double *mult,
                      const uint32_t *pend, uint64_t nroots, bcg_stats *stats);
 
+/* bcg_run_weighted for one root (mult, pend as there) that also writes the
+ * root's BFS depths level[n] (-1 = unreachable) in the same search: the
+ * per-source state the reference's driver reads back between its kernel
+ * calls (get_msk and pre_update_bc_cuda after scan_col_csc_cuda_mono,
+ * bc2d.c:504-580).  stats may be NULL.  Not available with BCG_PRUNE_TREES. */
+int bcg_run_root_levels(bcg_graph *g, uint32_t root, double mult, uint32_t pend, int32_t *level,
+                        bcg_stats *stats);
+
 /* Forces the sources-per-batch width (1, 3 or 6; 0 = automatic). */
 int bcg_set_batch_width(bcg_graph *g, uint32_t width);
 
