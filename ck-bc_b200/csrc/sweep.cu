@@ -533,7 +533,13 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
             else m |= (uint32_t)(L == dl) << k;
         }
         if (MODE == kFwdPull && vi.x == 0) m = 0;  // no edge: cannot be reached
-        if (m) {
+        // Forward sweeps index only the active vertices' edges (their sums
+        // are exact integers, so the grouping does not matter).  Backward
+        // sweeps index every vertex's edges (inactive ones are skipped when
+        // gathering): a vertex's run boundaries then depend on the tile alone,
+        // not on which other vertices the batch's other slots made active,
+        // so its FP64 sum is the same bits in any batch.
+        if (m || MODE == kBwd) {
             const uint32_t eb = hub ? T.e0 : ob;
             uint32_t ee = ob + vi.x;
             if (hub && T.e1 < ee) ee = T.e1;
@@ -591,11 +597,16 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
             base = ws.eb[j] - ws.pre[j];
         }
         const uint32_t jfirst = j, nfirst = nxt;
+        // uu[q]: the item's neighbour, or kSkipItem when its vertex has no
+        // active slot (backward sweeps index inactive vertices too)
+        constexpr uint32_t kSkipItem = 0xFFFFFFFFu;
         uint32_t uu[kItems];
+        uint32_t jm = (MODE == kBwd && has) ? ws.mask[j] : 1u;
+        bool any_act = false;
 #pragma unroll
         for (int q = 0; q < kItems; ++q) {
             const uint32_t i = i0 + q;
-            uu[q] = 0;
+            uu[q] = kSkipItem;
             if (i < i1) {
                 if (i >= nxt) {
                     do {
@@ -603,10 +614,16 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
                         nxt = ws.pre[j + 1];
                     } while (i >= nxt);
                     base = ws.eb[j] - ws.pre[j];
+                    if (MODE == kBwd) jm = ws.mask[j];
                 }
-                uu[q] = adjs[base + i];
+                if (jm) {
+                    uu[q] = adjs[base + i];
+                    any_act = true;
+                }
             }
         }
+        // a backward round none of whose vertices is active adds nothing
+        if (MODE == kBwd && !__any_sync(0xffffffffu, any_act)) continue;
         // the walk again while the loads are in flight: vertex of item i
         j = jfirst;
         nxt = nfirst;
@@ -676,7 +693,7 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
                 uint32_t wr[kHalf][NW];
 #pragma unroll
                 for (int q = 0; q < kHalf; ++q)
-                    if (i0 + h0 + q < i1) ld_row<NW>(row_of<S>(a, uu[h0 + q]), wr[q]);
+                    if (uu[h0 + q] != kSkipItem) ld_row<NW>(row_of<S>(a, uu[h0 + q]), wr[q]);
 #pragma unroll
                 for (int q = 0; q < kHalf; ++q) {
                     const int idx = h0 + q;
