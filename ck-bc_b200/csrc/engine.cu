@@ -619,6 +619,7 @@ int enqueue_packed(bcg_graph *g, const PackedRun &p, uint32_t S, cudaStream_t st
     a.xrbeg = p.xrbeg;
     a.xrange = p.xrange;
     a.xout = p.xout;
+    a.slot_delta = p.xout ? p.slot_delta : nullptr;
     int grid = 0;
     return launch_sweep((int)S, a, st, &grid);
 }

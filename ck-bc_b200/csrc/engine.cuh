@@ -5,20 +5,21 @@
 
 namespace bcg {
 
-// Sweep kernel geometry (one CTA per SM; the build may override both).  256
-// threads: each lane keeps the rows of a whole run (8 gathers of up to 32
-// bytes) in registers, about 250 registers per thread.
-#ifndef BCG_THREADS
-#define BCG_THREADS 256
-#endif
-constexpr int kThreads = BCG_THREADS;    // threads per CTA of the sweep kernel
-constexpr int kWarps = kThreads / 32;    // independent tile workers per CTA
+// Sweep kernel geometry (one CTA per SM).  Each lane keeps the rows of a
+// whole segment (kItems gathers of up to 32 bytes) in registers; 512 threads
+// leave 128 registers per thread, which widths 1 and 3 fit, and width 6 runs
+// with 384 threads (168 registers).
+template <int S>
+struct SweepGeom {
+    static constexpr int kThreads = (S == 6) ? 384 : 512;
+    static constexpr int kWarps = kThreads / 32;  // independent tile workers per CTA
+};
 constexpr int kTileVerts = 32;           // max vertices per tile (one per lane)
 #ifndef BCG_TILE_EDGES
 #define BCG_TILE_EDGES 512
 #endif
 constexpr int kTileEdges = BCG_TILE_EDGES;  // max adjacency entries per tile
-constexpr int kItems = 8;                   // edges per lane in one round of a tile
+constexpr int kItems = 4;                   // edges of a segment: one lane's share of a round
 constexpr int kRoundEdges = 32 * kItems;    // a warp takes a tile's edges in rounds of this many
 static_assert(kTileEdges % kRoundEdges == 0, "a tile holds whole rounds");
 constexpr int kPushSplit = 8;            // sparse push sweeps: warps per tile
@@ -165,9 +166,11 @@ struct BatchArgs {
     const uint32_t *xtiles;
     const uint32_t *xrbeg;
     const uint2 *xrange;
-    // served waves: xout[q] routes the slots of range q (ranges of a batch
-    // sorted by first tile); nullptr: dependencies go to bc as usual
+    // served waves: the backward pass keeps each slot's dependencies in
+    // slot_delta[k * n + v], and at the batch's end xout[q] routes the slots
+    // of range q into the requests' buffers; nullptr: dependencies go to bc
     const SlotOut *xout;
+    double *slot_delta;
 };
 
 }  // namespace bcg

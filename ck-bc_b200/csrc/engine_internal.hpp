@@ -96,6 +96,7 @@ struct PackedRun {
     const uint32_t *xtiles, *xrbeg;
     const uint2 *xrange;
     const bcg::SlotOut *xout;  // nullptr: dependencies into the union's bc
+    double *slot_delta;        // with xout: S * n doubles of per-slot dependencies
     uint32_t nbatch;
     RootStat *rstat;  // nbatch * S per-slot totals
 };

@@ -14,11 +14,12 @@
 // slots with its own sources).  Each graph takes up to wave_batches * S of
 // the not yet scheduled sources of ALL its admitted requests, oldest request
 // first, so requests on the same graph share the adjacency passes of a
-// batch.  The sweep kernel adds each slot's dependencies straight into the
-// buffer of the request that owns the slot's source (SlotOut routing), one
-// slot after the other: a request's sources reach its buffer in its own
-// source order however they are packed, so its result is bitwise the same
-// alone or in any mix.  S is 6 while the active graphs' 64-byte state rows
+// batch.  The sweep kernel keeps each slot's dependencies apart and, at the
+// end of every batch, adds them into the buffer of the request that owns the
+// slot's source (SlotOut routing), one slot after the other: a request's
+// sources reach its buffer in its own source order however they are packed,
+// and a source's dependencies do not depend on its batch-mates, so its
+// result is bitwise the same alone or in any mix.  S is 6 while the active graphs' 64-byte state rows
 // fit 64 MB (they then stay in L2), else 3.
 //
 // Continuity.  bcg_server_step never waits for the GPU: it retires the waves
@@ -87,6 +88,7 @@ struct bcg_server {
     ServeWave slot[kInFlight];
     std::deque<int> inflight;  // wave slots in launch order
     cudaStream_t stream = nullptr, result_stream = nullptr;
+    double *d_slot_delta = nullptr;  // width * n per-slot dependencies of a batch
     uint64_t waves = 0;
     int sticky_error = BCG_OK;  // a failed wave leaves the server unusable
 };
@@ -253,6 +255,7 @@ int enqueue_wave(bcg_server *s, bool *launched) {
         p.xrbeg = reinterpret_cast<const uint32_t *>(d + s->off_xrbeg);
         p.xrange = reinterpret_cast<const uint2 *>(d + s->off_xrange);
         p.xout = reinterpret_cast<const SlotOut *>(d + s->off_xout);
+        p.slot_delta = s->d_slot_delta;
         p.nbatch = nb;
         p.rstat = w.d_rstat;
         int rc = enqueue_packed(s->g, p, S, s->stream);
@@ -343,8 +346,10 @@ int bcg_server_create(uint32_t ngraphs, const uint32_t *const *offsets, const ui
             return fail(set_error(BCG_ERR_ARG, "the pool union does not keep the graphs in caller order"));
     rc = ensure_state(s->g, s->width);
     if (rc) return fail(rc);
+    if (cudaMalloc(&s->d_slot_delta, (size_t)s->width * s->g->n * sizeof(double)) != cudaSuccess)
+        return fail(set_error(BCG_ERR_OOM, "per-slot dependency buffer"));
     s->budget = hbm_budget_bytes;
-    s->resident = pool_bytes(s->g, s->width);
+    s->resident = pool_bytes(s->g, s->width) + (uint64_t)s->width * s->g->n * sizeof(double);
     if (s->resident > s->budget)
         return fail(set_error(BCG_ERR_OOM, "the resident pool needs %llu bytes, over the %llu-byte budget",
                               (unsigned long long)s->resident, (unsigned long long)s->budget));
@@ -397,6 +402,7 @@ int bcg_server_destroy(bcg_server *s) {
         }
         if (s->stream) cudaStreamDestroy(s->stream);
         if (s->result_stream) cudaStreamDestroy(s->result_stream);
+        cudaFree(s->d_slot_delta);
         if (s->g) bcg_graph_destroy(s->g);
     }
     delete s;

@@ -216,6 +216,7 @@ __device__ __forceinline__ unsigned long long *val_at(unsigned char *row, int k)
 // Adjacency entries a tile buffer holds: the range [e0, e1) widened to
 // 16-byte boundaries on both sides (<= 3 entries each).
 constexpr int kAdjBuf = kTileEdges + 8;
+
 static_assert((kAdjBuf * 4) % 16 == 0, "tile buffers keep 16-byte alignment");
 
 // Per-warp scratch.
@@ -226,13 +227,15 @@ struct WarpSmem {
     alignas(16) uint2 vbuf[2][kTileVerts + 2];   // their {degree, reach} words, from an even vertex on
     alignas(16) uint32_t obuf[2][kTileVerts + 8];  // their row starts, from a multiple-of-4 vertex on
     unsigned long long mbar[2];              // completion of the four copies of buffer b
-    uint32_t pre[kTileVerts + 1];            // exclusive scan of active degrees
-    uint32_t eb[kTileVerts];                 // start of vertex j's active edges in its adjs buffer
+    uint32_t pre[kTileVerts + 1];            // exclusive scan of the vertices' segment counts
+    uint32_t eb[kTileVerts];                 // start of vertex j's edges in its adjs buffer
+    uint32_t dg[kTileVerts];                 // vertex j's edges in this sweep (0: none)
     uint32_t mask[kTileVerts];               // active slots of vertex j
+    unsigned long long part[32][S];          // the round's segment partial sums, by lane
     uint32_t app[2 * 32];   // buffered appends to the next level's list
     uint32_t uapp[2 * 32];  // buffered appends to the unvisited-tile ring
     uint32_t napp, nuapp;
-    unsigned long long acc[kTileVerts][S];   // per-vertex sums of the tile (one writer per round)
+    unsigned long long acc[kTileVerts][S];   // per-vertex sums of the tile
     unsigned long long own[kTileVerts][S];   // push: sigma of the frontier vertex's active slots
     // per-warp discovery totals of the sweep (LaneCounts layout)
     unsigned long long cnt[2 + 3 * S];
@@ -240,7 +243,7 @@ struct WarpSmem {
 
 template <int S>
 struct Smem {
-    WarpSmem<S> w[kWarps];
+    WarpSmem<S> w[SweepGeom<S>::kWarps];
     // per-CTA counters of the current sweep
     unsigned long long c_disc, c_pf;
     unsigned long long c_vis[S], c_w[S], c_mc[S];
@@ -486,13 +489,19 @@ __device__ __forceinline__ void sigma_atomic(unsigned long long *p, unsigned lon
     }
 }
 
-__device__ __forceinline__ unsigned long long shfl_up64(unsigned long long v, int o) {
-    return __shfl_up_sync(0xffffffffu, v, o);
-}
-
 // One tile (or one part of a split tile), processed by one warp.  The tile's
 // adjacency (copied from entry T.e0 & ~3 on), own rows, degree/reach words
 // and row starts are in buffer `buf` of the warp's scratch (tile_fetch).
+//
+// Work split.  Every vertex's edges of the sweep are cut into segments of
+// kItems edges aligned to the vertex's first edge; each lane takes one
+// segment per round.  Forward sweeps count only the active vertices' edges;
+// backward sweeps count every vertex's (an inactive vertex's segments load
+// nothing), so a vertex's segments depend on the tile alone.  A lane adds its
+// segment's terms in adjacency order, and the segment partials of a vertex are
+// folded left to right in segment order by the vertex's own lane after every
+// round (in a one-vertex tile: lane-wise over the rounds, then over the lanes
+// by a fixed butterfly): the same bits whatever the batch's other slots did.
 template <int S, int MODE, bool EXT>
 __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint32_t ti, const Tile &T,
                           uint32_t part, const SweepCtx &x, int buf) {
@@ -505,7 +514,6 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
     const uint32_t nv = T.v1 - T.v0;
     const uint32_t *adjs = ws.adjs[buf];
     const uint32_t ab = T.e0 & ~3u;
-    uint32_t deg_act = 0, m = 0;
     // the lane's own row, as copied with the tile (levels, and sigma of the
     // slots whose level is d); read again from the buffer where needed
     auto own_row = [&](uint32_t (&ow)[NW]) {
@@ -522,7 +530,8 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
         vi = ws.vbuf[buf][(T.v0 & 1u) + lane];
         ob = ws.obuf[buf][(T.v0 & 3u) + lane];
     }
-    // ---- phase 1: the lane's vertex (its data arrived with the tile)
+    // ---- phase 1: the lane's vertex
+    uint32_t m = 0, dg = 0;
     if (lane < nv) {
         uint32_t ow[NW];
         own_row(ow);
@@ -533,123 +542,80 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
             else m |= (uint32_t)(L == dl) << k;
         }
         if (MODE == kFwdPull && vi.x == 0) m = 0;  // no edge: cannot be reached
-        // Forward sweeps index only the active vertices' edges (their sums
-        // are exact integers, so the grouping does not matter).  Backward
-        // sweeps index every vertex's edges (inactive ones are skipped when
-        // gathering): a vertex's run boundaries then depend on the tile alone,
-        // not on which other vertices the batch's other slots made active,
-        // so its FP64 sum is the same bits in any batch.
-        if (m || MODE == kBwd) {
-            const uint32_t eb = hub ? T.e0 : ob;
-            uint32_t ee = ob + vi.x;
-            if (hub && T.e1 < ee) ee = T.e1;
-            if (ee < eb) ee = eb;
-            deg_act = ee - eb;
-            if (MODE == kBwd && d == x.D) deg_act = 0;
-            ws.eb[lane] = eb - ab;
-            if (MODE != kFwdPush) {
+        const uint32_t eb = hub ? T.e0 : ob;
+        uint32_t ee = ob + vi.x;
+        if (hub && T.e1 < ee) ee = T.e1;
+        if (ee < eb) ee = eb;
+        if (m || MODE == kBwd) dg = ee - eb;
+        if (MODE == kBwd && d == x.D) dg = 0;
+        ws.eb[lane] = eb - ab;
+        ws.dg[lane] = dg;
+        if (MODE == kFwdPush) {
 #pragma unroll
-                for (int k = 0; k < S; ++k) ws.acc[lane][k] = 0ull;
-            } else {
-#pragma unroll
-                for (int k = 0; k < S; ++k) ws.own[lane][k] = ((m >> k) & 1u) ? w_val<S>(ow, k) : 0ull;
-            }
+            for (int k = 0; k < S; ++k) ws.own[lane][k] = ((m >> k) & 1u) ? w_val<S>(ow, k) : 0ull;
         }
         ws.mask[lane] = m;
     }
     if (hub && !__shfl_sync(0xffffffffu, m, 0)) return;  // same decision in every chunk
-    uint32_t incl = deg_act;
+    // segment prefix
+    const uint32_t nseg = (dg + kItems - 1) / kItems;
+    uint32_t incl = nseg;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= (unsigned)o) incl += y;
     }
     const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-    if (lane < nv) ws.pre[lane] = incl - deg_act;
+    if (lane < nv) ws.pre[lane] = incl - nseg;
     if (lane == 0) ws.pre[nv] = total;
     __syncwarp();
 
-    // ---- phase 2: this part's edges [w0, w1), in rounds of <= kRoundEdges;
-    // in each round every lane takes a contiguous run of <= kItems
-    uint32_t w0 = 0, w1 = total;
+    // ---- phase 2: segments [s0, s1) of this part, one per lane per round
+    uint32_t s0 = 0, s1 = total;
     if (MODE == kFwdPush && x.split > 1) {
-        w0 = (uint32_t)(((unsigned long long)total * part) / x.split);
-        w1 = (uint32_t)(((unsigned long long)total * (part + 1)) / x.split);
+        s0 = (uint32_t)(((unsigned long long)total * part) / x.split);
+        s1 = (uint32_t)(((unsigned long long)total * (part + 1)) / x.split);
     }
-    for (uint32_t r0 = w0; r0 < w1; r0 += kRoundEdges) {
-        const uint32_t r1 = min(w1, r0 + (uint32_t)kRoundEdges);
-        const uint32_t per = (r1 - r0 + 31) / 32;  // <= kItems
-        const uint32_t i0 = r0 + lane * per;
-        const uint32_t i1 = min(r1, i0 + per);
-        const bool has = i0 < i1;
-        // the run's vertex j, the end of its edges (nxt) and the offset of its
-        // edges in adjs (base + i) stay in registers; they are reloaded from
-        // shared memory only when the run crosses into the next vertex
-        uint32_t j = 0, nxt = 0, base = 0;
+    constexpr uint32_t kSkipItem = 0xFFFFFFFFu;
+    // one-vertex tiles keep their partials in registers, summed round by round
+    const bool solo = (nv == 1);
+    unsigned long long ls[S];
+#pragma unroll
+    for (int k = 0; k < S; ++k) ls[k] = 0ull;
+    // the lane's own vertex: its segments and the running fold of their sums
+    const uint32_t myp0 = (lane < nv) ? ws.pre[lane] : 0u, myp1 = (lane < nv) ? ws.pre[lane + 1] : 0u;
+    for (uint32_t r0 = s0; r0 < s1; r0 += 32) {
+        const uint32_t seg = r0 + lane;
+        const bool has = seg < s1;
+        uint32_t j = 0, cnt = 0, e0 = 0, jm = 0;
         if (has) {
             uint32_t lo = 0, hi = nv;
             while (hi - lo > 1) {
                 const uint32_t mid = (lo + hi) >> 1;
-                if (ws.pre[mid] <= i0) lo = mid; else hi = mid;
+                if (ws.pre[mid] <= seg) lo = mid; else hi = mid;
             }
             j = lo;
-            nxt = ws.pre[j + 1];
-            base = ws.eb[j] - ws.pre[j];
+            const uint32_t rr = (seg - ws.pre[j]) * kItems;
+            cnt = min((uint32_t)kItems, ws.dg[j] - rr);
+            e0 = ws.eb[j] + rr;
+            jm = ws.mask[j];
         }
-        const uint32_t jfirst = j, nfirst = nxt;
-        // uu[q]: the item's neighbour, or kSkipItem when its vertex has no
-        // active slot (backward sweeps index inactive vertices too)
-        constexpr uint32_t kSkipItem = 0xFFFFFFFFu;
+        if (MODE == kBwd && !__any_sync(0xffffffffu, jm != 0)) continue;  // nothing active in this round
         uint32_t uu[kItems];
-        uint32_t jm = (MODE == kBwd && has) ? ws.mask[j] : 1u;
-        bool any_act = false;
 #pragma unroll
-        for (int q = 0; q < kItems; ++q) {
-            const uint32_t i = i0 + q;
-            uu[q] = kSkipItem;
-            if (i < i1) {
-                if (i >= nxt) {
-                    do {
-                        ++j;
-                        nxt = ws.pre[j + 1];
-                    } while (i >= nxt);
-                    base = ws.eb[j] - ws.pre[j];
-                    if (MODE == kBwd) jm = ws.mask[j];
-                }
-                if (jm) {
-                    uu[q] = adjs[base + i];
-                    any_act = true;
-                }
-            }
-        }
-        // a backward round none of whose vertices is active adds nothing
-        if (MODE == kBwd && !__any_sync(0xffffffffu, any_act)) continue;
-        // the walk again while the loads are in flight: vertex of item i
-        j = jfirst;
-        nxt = nfirst;
-        auto vertex_of = [&](uint32_t i) -> uint32_t {
-            if (i >= nxt) {
-                do {
-                    ++j;
-                    nxt = ws.pre[j + 1];
-                } while (i >= nxt);
-            }
-            return j;
-        };
+        for (int q = 0; q < kItems; ++q) uu[q] = ((uint32_t)q < cnt && jm) ? adjs[e0 + q] : kSkipItem;
         if (MODE == kFwdPush) {
             // the targets' level blocks, then claim / add with atomics
             constexpr int NL = RowGeom<S>::kLvlBytes / 4;
-            LaneCounts<S> cnt;
+            LaneCounts<S> lc;
             uint32_t lw[kItems][NL];
 #pragma unroll
             for (int q = 0; q < kItems; ++q)
-                if (i0 + q < i1) ld_lvl<NL>(row_of<S>(a, uu[q]), lw[q]);
+                if (uu[q] != kSkipItem) ld_lvl<NL>(row_of<S>(a, uu[q]), lw[q]);
 #pragma unroll
             for (int q = 0; q < kItems; ++q) {
                 uint32_t app = kNoTile;
-                if (i0 + q < i1) {
-                    const uint32_t jq = vertex_of(i0 + q);
-                    const uint32_t jm = ws.mask[jq];
+                if (uu[q] != kSkipItem) {
                     const uint32_t wv = uu[q];
                     unsigned char *wrow = row_of<S>(a, wv);
                     bool claimed_any = false;
@@ -662,32 +628,29 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
                             const uint16_t old = atomicCAS(reinterpret_cast<unsigned short *>(lvl_at(wrow, k)),
                                                            (unsigned short)kUnvisited, (unsigned short)(d + 1));
                             if (old == kUnvisited) {
-                                cnt.add(k, a.vinfo[wv]);
+                                lc.add(k, a.vinfo[wv]);
                                 take = true;
                                 claimed_any = true;
                             } else {
                                 take = (old == (uint16_t)(d + 1));
                             }
                         }
-                        if (take) sigma_atomic<EXT>(val_at<S>(wrow, k), ws.own[jq][k], a);
+                        if (take) sigma_atomic<EXT>(val_at<S>(wrow, k), ws.own[j][k], a);
                     }
                     if (claimed_any) app = claim_tile(a, wv, x.key_next);
                 }
                 append_level<S>(a, ws, app, x);
             }
-            flush_counts<S>(ws, cnt);
+            flush_counts<S>(ws, lc);
         } else {
             // gather the neighbours' rows (kHalf at a time: all 8 for rows of
             // up to 32 bytes, 4 for 64-byte rows) and sum the matching values
-            // of each vertex in adjacency order
+            // in adjacency order
             constexpr int kHalf = (NW <= 8) ? kItems : kItems / 2;
             const uint16_t want = (MODE == kFwdPull) ? dl : (uint16_t)(d + 1);
-            unsigned long long run[S], head[S];
+            unsigned long long run[S];
 #pragma unroll
-            for (int k = 0; k < S; ++k) { run[k] = 0ull; head[k] = 0ull; }
-            uint32_t runj = jfirst;
-            uint32_t runm = has ? ws.mask[runj] : 0u;
-            bool split_run = false;  // the run has left its first vertex (head[] holds its part)
+            for (int k = 0; k < S; ++k) run[k] = 0ull;
 #pragma unroll
             for (int h0 = 0; h0 < kItems; h0 += kHalf) {
                 uint32_t wr[kHalf][NW];
@@ -696,75 +659,54 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
                     if (uu[h0 + q] != kSkipItem) ld_row<NW>(row_of<S>(a, uu[h0 + q]), wr[q]);
 #pragma unroll
                 for (int q = 0; q < kHalf; ++q) {
-                    const int idx = h0 + q;
-                    if (i0 + idx >= i1) continue;
-                    const uint32_t jq = vertex_of(i0 + idx);
-                    if (jq != runj) {
-                        if (!split_run) {
-#pragma unroll
-                            for (int k = 0; k < S; ++k) head[k] = run[k];
-                            split_run = true;
-                        } else {
-                            // a vertex wholly inside this lane's run: its round total
-#pragma unroll
-                            for (int k = 0; k < S; ++k) ws.acc[runj][k] = vsum<EXT, MODE>(ws.acc[runj][k], run[k], a);
-                        }
-#pragma unroll
-                        for (int k = 0; k < S; ++k) run[k] = 0ull;
-                        runj = jq;
-                        runm = ws.mask[runj];
-                    }
+                    if (uu[h0 + q] == kSkipItem) continue;
 #pragma unroll
                     for (int k = 0; k < S; ++k) {
-                        if (!((runm >> k) & 1u) || w_lvl(wr[q], k) != want) continue;
+                        if (!((jm >> k) & 1u) || w_lvl(wr[q], k) != want) continue;
                         run[k] = vsum<EXT, MODE>(run[k], w_val<S>(wr[q], k), a);
                     }
                 }
             }
-            // Partial sums of vertices that span lanes, combined in lane
-            // order: a segmented inclusive scan of the run tails keyed by
-            // their vertex (keys do not decrease with the lane).
-            const uint32_t key_last = has ? runj : 0xFFFFFFFFu;
-            const uint32_t key_first = has ? jfirst : 0xFFFFFFFEu;
-            unsigned long long sc[S];
+            if (solo) {
 #pragma unroll
-            for (int k = 0; k < S; ++k) sc[k] = run[k];
+                for (int k = 0; k < S; ++k) ls[k] = vsum<EXT, MODE>(ls[k], run[k], a);
+            } else {
+                if (has) {
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t ko = __shfl_up_sync(0xffffffffu, key_last, o);
-                const bool same = lane >= (unsigned)o && ko == key_last;
-#pragma unroll
-                for (int k = 0; k < S; ++k) {
-                    const unsigned long long y = shfl_up64(sc[k], o);
-                    if (same) sc[k] = vsum<EXT, MODE>(y, sc[k], a);
+                    for (int k = 0; k < S; ++k) ws.part[lane][k] = run[k];
                 }
+                __syncwarp();
+                // each vertex's lane folds in its segments of this round, in order
+                const uint32_t q0 = max(myp0, r0), q1 = min(myp1, r0 + 32u);
+                for (uint32_t q = q0; q < q1; ++q) {
+#pragma unroll
+                    for (int k = 0; k < S; ++k) ls[k] = vsum<EXT, MODE>(ls[k], ws.part[q - r0][k], a);
+                }
+                __syncwarp();
             }
-            const uint32_t kprev = __shfl_up_sync(0xffffffffu, key_last, 1);
-            const uint32_t knext = __shfl_down_sync(0xffffffffu, key_first, 1);
-            const bool carry_in = lane > 0 && kprev == key_first;
-            unsigned long long carry[S];
-#pragma unroll
-            for (int k = 0; k < S; ++k) carry[k] = shfl_up64(sc[k], 1);
-            if (has) {
-                if (split_run) {
-                    // the run's first vertex ends in this lane: earlier lanes' part, then this one's
-#pragma unroll
-                    for (int k = 0; k < S; ++k) {
-                        const unsigned long long t = carry_in ? vsum<EXT, MODE>(carry[k], head[k], a) : head[k];
-                        ws.acc[jfirst][k] = vsum<EXT, MODE>(ws.acc[jfirst][k], t, a);
-                    }
-                }
-                if (lane == 31 || knext != key_last) {
-                    // the last lane holding the run's last vertex adds the vertex's round total
-#pragma unroll
-                    for (int k = 0; k < S; ++k) ws.acc[key_last][k] = vsum<EXT, MODE>(ws.acc[key_last][k], sc[k], a);
-                }
-            }
-            __syncwarp();
         }
     }
     __syncwarp();
     if (MODE == kFwdPush) return;
+
+    // ---- each vertex's total over its segments, in segment order
+    if (solo) {
+        // lane l held segments l, l + 32, ... (rounds in order); the lanes'
+        // sums meet in a fixed butterfly, every lane ending with the total
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) {
+#pragma unroll
+            for (int k = 0; k < S; ++k) ls[k] = vsum<EXT, MODE>(ls[k], __shfl_xor_sync(0xffffffffu, ls[k], o), a);
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < S; ++k) ws.acc[0][k] = ls[k];
+        }
+    } else if (lane < nv) {
+#pragma unroll
+        for (int k = 0; k < S; ++k) ws.acc[lane][k] = ls[k];
+    }
+    __syncwarp();
 
     // ---- hub chunks: each chunk stores its total in its own slot; the chunk
     // that arrives last adds the slots in chunk order and finishes the vertex
@@ -812,16 +754,6 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
             const double reach = (double)vi.y;
             uint32_t ow[NW];
             own_row(ow);
-            // served waves: the slots' own result buffers for this tile's graph
-            const SlotOut *xo = nullptr;
-            if (a.xout) {
-                uint32_t lo = a.xrbeg[x.b], hi = a.xrbeg[x.b + 1];
-                while (hi - lo > 1) {
-                    const uint32_t mid = (lo + hi) >> 1;
-                    if (a.xrange[mid].x <= ti) lo = mid; else hi = mid;
-                }
-                xo = a.xout + lo;
-            }
 #pragma unroll
             for (int k = 0; k < S; ++k) {
                 if (!((m >> k) & 1u)) continue;
@@ -840,18 +772,14 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
                     *val_at<S>(vrow, k) = (unsigned long long)__double_as_longlong(xo);
                 }
                 if (d > 0) {
-                    if (xo) {
-                        // one add per slot, slots in order: a request's sources
-                        // reach its buffer in source order however they are packed
-                        double *o = xo->out[k];
-                        if (o) o[v - xo->base] += delta;
-                    } else {
-                        add += sm.mult[k] * delta;
-                    }
+                    // served waves keep each slot's dependencies apart (added
+                    // to the requests in slot order at the batch's end)
+                    if (a.slot_delta) a.slot_delta[(size_t)k * a.n + v] = delta;
+                    else add += sm.mult[k] * delta;
                 }
                 if (a.dbg_delta) a.dbg_delta[(size_t)k * a.n + v] = delta;
             }
-            if (d > 0 && !xo) a.bc[a.ext ? a.ext[v] : v] += add;
+            if (d > 0 && !a.slot_delta) a.bc[a.ext ? a.ext[v] : v] += add;
         }
     }
     if (MODE == kFwdPull) {
@@ -1025,7 +953,7 @@ __device__ __forceinline__ void run_sweep(const BatchArgs &a, Smem<S> &sm, const
 }
 
 template <int S, bool EXT>
-__global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
+__global__ void __launch_bounds__(SweepGeom<S>::kThreads, 1) bc_sweep_kernel(BatchArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     Smem<S> &sm = *reinterpret_cast<Smem<S> *>(smem_raw);
     constexpr int R = RowGeom<S>::kBytes;
@@ -1033,7 +961,7 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
     const unsigned int nblk = gridDim.x;
     const unsigned long long wait_ns = c->wait_ns ? c->wait_ns : kDefaultWaitNs;
     const unsigned long long ring = 2ull * a.ntiles;
-    const uint32_t total_warps = gridDim.x * kWarps;
+    const uint32_t total_warps = gridDim.x * SweepGeom<S>::kWarps;
     {
         WarpSmem<S> &ws = sm.w[threadIdx.x >> 5];
         if ((threadIdx.x & 31) == 0) {
@@ -1282,6 +1210,31 @@ __global__ void __launch_bounds__(kThreads, 1) bc_sweep_kernel(BatchArgs a) {
             trace(a, b, 3u, (uint32_t)dd, lc, 0);
         }
 
+        // ---- served waves: each slot's dependencies into the buffer of the
+        // request that owns the slot's source, slots in order (so a request's
+        // sources reach its buffer in source order however they were packed)
+        if (a.slot_delta) {
+            const uint32_t q0 = a.xrbeg[b], q1 = a.xrbeg[b + 1];
+            for (uint32_t q = q0; q < q1; ++q) {
+                const uint2 rg = a.xrange[q];
+                const uint32_t len = ((q + 1 < q1) ? a.xrange[q + 1].y : a.xtiles[b]) - rg.y;
+                if (!len) continue;
+                const SlotOut o = a.xout[q];
+                const size_t v0 = a.tiles[rg.x].v0, v1 = a.tiles[rg.x + len - 1].v1;
+                for (size_t v = v0 + (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < v1;
+                     v += (size_t)gridDim.x * blockDim.x) {
+                    const unsigned char *row = a.rows + v * R;
+#pragma unroll
+                    for (int k = 0; k < S; ++k) {
+                        const uint16_t L = *reinterpret_cast<const uint16_t *>(row + 2 * k);
+                        if (L == kUnvisited || L == 0 || !o.out[k]) continue;
+                        o.out[k][v - o.base] += a.slot_delta[(size_t)k * a.n + v];
+                    }
+                }
+            }
+            if (!grid_sync(c, nblk, wait_ns)) return;
+        }
+
         // ---- source term and per-root statistics
         if (blockIdx.x == 0 && threadIdx.x < S) {
             const int k = threadIdx.x;
@@ -1314,14 +1267,15 @@ static int launch_impl(const BatchArgs &a, cudaStream_t st, int *grid_out) {
     int dev = 0, nsm = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bc_sweep_kernel<S, EXT>, kThreads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bc_sweep_kernel<S, EXT>, SweepGeom<S>::kThreads, smem);
     if (e != cudaSuccess) return set_error(BCG_ERR_CUDA, "occupancy query: %s", cudaGetErrorString(e));
     if (per_sm < 1) return set_error(BCG_ERR_CUDA, "sweep kernel cannot be resident (smem %zu)", smem);
     int grid = nsm * per_sm;
     if (grid_out) *grid_out = grid;
     BatchArgs args = a;
     void *params[] = {&args};
-    e = cudaLaunchCooperativeKernel((const void *)bc_sweep_kernel<S, EXT>, dim3(grid), dim3(kThreads), params, smem, st);
+    e = cudaLaunchCooperativeKernel((const void *)bc_sweep_kernel<S, EXT>, dim3(grid), dim3(SweepGeom<S>::kThreads), params, smem,
+                                    st);
     if (e != cudaSuccess)
         return set_error(e == cudaErrorNoKernelImageForDevice ? BCG_ERR_NOGPU : BCG_ERR_CUDA,
                          "sweep kernel launch: %s", cudaGetErrorString(e));
