@@ -134,8 +134,9 @@ def test_pruning_edge_cases():
 
 
 def test_hub_chunks_all_modes():
-    # vertex 0 adjacent to 9000 vertices (more than one 4096-entry tile) plus a
-    # ring through them: exercises split hubs in push, pull and backward sweeps
+    # vertex 0 adjacent to 9000 vertices (18 chunks of 512 adjacency entries)
+    # plus a path through them: exercises split hubs in push, pull and
+    # backward sweeps
     k = 9000
     pairs = [[0, i] for i in range(1, k + 1)] + [[i, i + 1] for i in range(1, k)] + [[k, k + 1], [k + 1, k + 2]]
     n = k + 3
