@@ -232,21 +232,22 @@ static int ensure_run(bcg_graph *g, size_t slots) {
     return BCG_OK;
 }
 
-// Sources per batch: the widest S in {6, 3, 1} whose state rows
-// (n * row_bytes(S)) fit the budget that keeps them L2-resident, and not
-// wider than the number of roots needs.
+// Sources per batch: the widest S in {6, 3, 1} whose state rows (one per
+// searched vertex, row_bytes(S) each) fit the budget that keeps them
+// L2-resident, and not wider than the number of roots needs.
 static uint32_t choose_width(const bcg_graph *g, uint64_t nroots) {
     if (g->forced_width) return g->forced_width;
     double budget = 64.0 * 1024 * 1024;
     if (const char *e = getenv("BCG_STATE_BUDGET_MB")) budget = atof(e) * 1024 * 1024;
+    const double nrows = g->tile_n ? g->tile_n : g->n;  // pendant-tree mode searches the kept vertices only
     // low-degree graphs (mean degree below 6: grids, meshes, long chains) have
     // small frontiers and many levels, so sweeps cost barriers, not gathers,
     // and the widest batch wins whether or not the rows fit L2 (measured on a
     // 2048 x 2048 grid: 0.11 / 0.20 / 0.22 G TEPS at widths 1 / 3 / 6)
-    if ((double)g->nnz_pruned < 6.0 * g->n) budget = 1e30;
+    if ((double)g->nnz_pruned < 6.0 * nrows) budget = 1e30;
     uint32_t S = 6;
-    if ((double)g->n * row_bytes(6) > budget || nroots <= 3) S = 3;
-    if (S == 3 && ((double)g->n * row_bytes(3) > budget || nroots <= 1)) S = 1;
+    if (nrows * row_bytes(6) > budget || nroots <= 3) S = 3;
+    if (S == 3 && (nrows * row_bytes(3) > budget || nroots <= 1)) S = 1;
     return S;
 }
 

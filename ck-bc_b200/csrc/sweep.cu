@@ -232,6 +232,7 @@ struct WarpSmem {
     uint32_t dg[kTileVerts];                 // vertex j's edges in this sweep (0: none)
     uint32_t mask[kTileVerts];               // active slots of vertex j
     unsigned long long part[32][S];          // the round's segment partial sums, by lane
+    unsigned char sown[kTileEdges / kItems + kTileVerts];  // vertex of each segment of the tile
     uint32_t app[2 * 32];   // buffered appends to the next level's list
     uint32_t uapp[2 * 32];  // buffered appends to the unvisited-tile ring
     uint32_t napp, nuapp;
@@ -493,12 +494,12 @@ __device__ __forceinline__ void sigma_atomic(unsigned long long *p, unsigned lon
 // adjacency (copied from entry T.e0 & ~3 on), own rows, degree/reach words
 // and row starts are in buffer `buf` of the warp's scratch (tile_fetch).
 //
-// Work split.  Every vertex's edges of the sweep are cut into segments of
-// kItems edges aligned to the vertex's first edge; each lane takes one
-// segment per round.  Forward sweeps count only the active vertices' edges;
-// backward sweeps count every vertex's (an inactive vertex's segments load
-// nothing), so a vertex's segments depend on the tile alone.  A lane adds its
-// segment's terms in adjacency order, and the segment partials of a vertex are
+// Work split.  Every active vertex's edges are cut into segments of kItems
+// edges aligned to the vertex's first edge; each lane takes one segment per
+// round (its vertex from a per-tile segment map).  A vertex's segments
+// depend on the vertex alone, not on which other vertices are active.  A
+// lane adds its segment's terms in adjacency order, and the segment partials
+// of a vertex are
 // folded left to right in segment order by the vertex's own lane after every
 // round (in a one-vertex tile: lane-wise over the rounds, then over the lanes
 // by a fixed butterfly): the same bits whatever the batch's other slots did.
@@ -546,7 +547,7 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
         uint32_t ee = ob + vi.x;
         if (hub && T.e1 < ee) ee = T.e1;
         if (ee < eb) ee = eb;
-        if (m || MODE == kBwd) dg = ee - eb;
+        if (m) dg = ee - eb;
         if (MODE == kBwd && d == x.D) dg = 0;
         ws.eb[lane] = eb - ab;
         ws.dg[lane] = dg;
@@ -568,6 +569,9 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
     const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
     if (lane < nv) ws.pre[lane] = incl - nseg;
     if (lane == 0) ws.pre[nv] = total;
+    // segment -> vertex map (one-vertex tiles need none)
+    if (nv > 1)
+        for (uint32_t p = incl - nseg; p < incl; ++p) ws.sown[p] = (unsigned char)lane;
     __syncwarp();
 
     // ---- phase 2: segments [s0, s1) of this part, one per lane per round
@@ -589,18 +593,12 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
         const bool has = seg < s1;
         uint32_t j = 0, cnt = 0, e0 = 0, jm = 0;
         if (has) {
-            uint32_t lo = 0, hi = nv;
-            while (hi - lo > 1) {
-                const uint32_t mid = (lo + hi) >> 1;
-                if (ws.pre[mid] <= seg) lo = mid; else hi = mid;
-            }
-            j = lo;
+            j = solo ? 0u : ws.sown[seg];
             const uint32_t rr = (seg - ws.pre[j]) * kItems;
             cnt = min((uint32_t)kItems, ws.dg[j] - rr);
             e0 = ws.eb[j] + rr;
             jm = ws.mask[j];
         }
-        if (MODE == kBwd && !__any_sync(0xffffffffu, jm != 0)) continue;  // nothing active in this round
         uint32_t uu[kItems];
 #pragma unroll
         for (int q = 0; q < kItems; ++q) uu[q] = ((uint32_t)q < cnt && jm) ? adjs[e0 + q] : kSkipItem;
@@ -648,6 +646,16 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
             // in adjacency order
             constexpr int kHalf = (NW <= 8) ? kItems : kItems / 2;
             const uint16_t want = (MODE == kFwdPull) ? dl : (uint16_t)(d + 1);
+            bool ovf = false;  // a wrapped uint64 sum (flagged once per round)
+            auto add = [&](unsigned long long x, unsigned long long y) -> unsigned long long {
+                if (EXT) return ext_add(x, y);
+                if (MODE == kBwd)
+                    return (unsigned long long)__double_as_longlong(__longlong_as_double((long long)x) +
+                                                                    __longlong_as_double((long long)y));
+                const unsigned long long t = x + y;
+                ovf |= t < y;
+                return t;
+            };
             unsigned long long run[S];
 #pragma unroll
             for (int k = 0; k < S; ++k) run[k] = 0ull;
@@ -663,10 +671,11 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
 #pragma unroll
                     for (int k = 0; k < S; ++k) {
                         if (!((jm >> k) & 1u) || w_lvl(wr[q], k) != want) continue;
-                        run[k] = vsum<EXT, MODE>(run[k], w_val<S>(wr[q], k), a);
+                        run[k] = add(run[k], w_val<S>(wr[q], k));
                     }
                 }
             }
+            if (!EXT && MODE != kBwd && ovf) flag_overflow(a.ctrl);
             if (solo) {
 #pragma unroll
                 for (int k = 0; k < S; ++k) ls[k] = vsum<EXT, MODE>(ls[k], run[k], a);
