@@ -293,9 +293,18 @@ __global__ void k_uf_link(uint32_t nlive, const uint32_t *__restrict__ offs2, co
     }
 }
 
+// After linking every root is final.  The walk here stores nothing on the
+// way (a path-halving store from one thread could land on root[v] after v's
+// own thread wrote the final root and put back an interior ancestor), so
+// root[v] is written once, by v's thread, with its root; a concurrent walk
+// that reads it sees either v's old parent or the root, both on v's path.
 __global__ void k_uf_flatten(uint32_t n, uint32_t *root) {
     const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v < n) root[v] = uf_find(root, v);
+    if (v >= n) return;
+    volatile uint32_t *r = root;
+    uint32_t cur = v, next;
+    while ((next = r[cur]) != cur) cur = next;
+    root[v] = cur;
 }
 
 // Component of every vertex (its anchor's root, an internal id) and the
