@@ -70,10 +70,13 @@ struct Ctrl {
     int error;      // BCG_ERR_* code set by the device, 0 = fine
     int overflow;   // a uint64 sigma sum wrapped
     unsigned long long wait_ns;  // bound of every device-side wait
-    unsigned long long uctr;     // monotone write position in the unvisited-tile ring
-    // ring of per-sweep counters, indexed by sweep % 4
+    // ring of per-sweep counters, indexed by sweep % 4: a sweep adds only to
+    // its own entry, and the entry is cleared two sweeps ahead, so a value
+    // read after the sweep's barrier cannot change while a faster CTA is
+    // already in the next sweep
     unsigned long long disc[4];  // (vertex, slot) pairs discovered in the sweep
     unsigned long long pf[4];    // sum of degrees over those pairs
+    unsigned long long uadd[4];  // tiles the sweep (a pull) appended to the unvisited-tile ring
     // per-slot accumulators of the current batch
     unsigned long long visited[8];
     unsigned long long wsum[8];  // sum of (1 + reach) over visited vertices

@@ -34,30 +34,37 @@
 // consecutive vertices and <= kTileEdges (512) adjacency entries; a vertex
 // with more entries is split into kTileEdges-entry chunks ("hub" chunks).
 // One warp works on one tile at a time with no CTA-wide synchronisation: lane
-// j owns vertex j, the tile's active edges are taken in rounds of <= 256, and
-// each round is cut into contiguous runs of <= 8 per lane (merge-path over the
-// warp's exclusive scan of active degrees).  Each warp pipelines its tiles:
-// while it works on one tile, the next tile's adjacency range is already
-// being copied into the other half of its shared buffer by one bulk
-// asynchronous copy (cp.async.bulk, completion on an mbarrier), and the next
-// tile's own rows, degree/reach words and row starts are in flight to
-// registers.  A tile then costs one dependent round trip per round (the row
-// gathers) instead of one more for its own data.  Push and backward sweeps
-// walk only the tiles on the level's list (tiles holding a vertex first
-// reached at that level, for any slot; a sparse push splits each tile over
-// kPushSplit warps); pull sweeps walk the tiles that still hold an unvisited
-// vertex (all tiles in the first pull of a batch).
+// j owns vertex j, every active vertex's edges are cut into segments of
+// kItems (4) edges aligned to the vertex's first edge, and the lanes take one
+// segment each per round (32 segments a round).  Each warp pipelines its
+// tiles: while it works on one tile, the next tile's adjacency range, own
+// rows, degree/reach words and row starts are already being copied into the
+// other half of its shared buffers by four 1-D bulk asynchronous copies
+// (cp.async.bulk, completion on an mbarrier), and the descriptors of the two
+// tiles after it are in registers.  A tile then costs one dependent round
+// trip per round (the row gathers) instead of more for its own data.  Push
+// and backward sweeps walk only the tiles on the level's list (tiles holding
+// a vertex first reached at that level, for any slot; a sparse push splits
+// each tile over kPushSplit warps); pull sweeps walk the tiles that still
+// hold an unvisited vertex (all tiles in the first pull of a batch).
 //
 // Deterministic sums.  A vertex's sum over its neighbours (sigma of parents
 // in a pull, X of children in the backward pass) is formed in a fixed order:
-// each lane adds its run's terms in adjacency order; the partial sums of a
-// vertex whose edges span several lanes are combined by a segmented warp scan
-// in lane order; the per-round totals are added into the vertex's shared
-// accumulator by the single lane that ends the vertex in that round, rounds
-// in order; a hub's chunk totals are stored in one slot per chunk and added in
-// chunk order by the chunk that arrives last.  No floating-point atomics are
+// each lane adds its segment's terms in adjacency order; the vertex's own
+// lane folds its segment partials left to right after every round; a
+// one-vertex tile sums lane-wise over the rounds and then over the lanes in
+// a fixed butterfly; a hub's chunk totals are stored in one slot per chunk
+// and added in chunk order by the chunk that arrives last.  The segments of
+// a vertex depend on that vertex alone, and no floating-point atomics are
 // used, so a run's results are bitwise reproducible and a source's
 // contribution does not depend on the batch it shares.
+//
+// Memory coherence.  The L1 caches of the SMs are not coherent with each
+// other: a plain load can hit a line this SM cached in an earlier sweep or
+// batch after another SM rewrote it in L2.  Everything that other SMs rewrite
+// during a launch (state rows, level lists, the unvisited ring, bc, hub
+// slots, tile marks) is therefore read with L2 loads (.cg, volatile or atomic)
+// or copied by the bulk-copy engine, which reads L2.
 #include <cstdio>
 
 #include "bcg.h"
@@ -79,6 +86,12 @@ __device__ __forceinline__ unsigned long long vload64(const unsigned long long *
 
 __device__ __forceinline__ uint32_t vload32(const uint32_t *p) {
     return *reinterpret_cast<const volatile uint32_t *>(p);
+}
+
+__device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
 }
 
 // L2 policy for streamed data: evicted before the state rows.
@@ -135,11 +148,11 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, uint32_t pari
 template <int NW>
 __device__ __forceinline__ void ld_row(const unsigned char *row, uint32_t (&w)[NW]) {
     if (NW == 4) {
-        asm volatile("ld.global.v4.u32 {%0,%1,%2,%3}, [%4];" : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]) : "l"(row));
+        asm volatile("ld.global.cg.v4.u32 {%0,%1,%2,%3}, [%4];" : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]) : "l"(row));
     } else {
 #pragma unroll
         for (int h = 0; h < NW / 8; ++h)
-            asm volatile("ld.global.v8.u32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+            asm volatile("ld.global.cg.v8.u32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
                          : "=r"(w[8 * h]), "=r"(w[8 * h + 1]), "=r"(w[8 * h + 2]), "=r"(w[8 * h + 3]), "=r"(w[8 * h + 4]),
                            "=r"(w[8 * h + 5]), "=r"(w[8 * h + 6]), "=r"(w[8 * h + 7])
                          : "l"(row + 32 * h));
@@ -149,9 +162,9 @@ __device__ __forceinline__ void ld_row(const unsigned char *row, uint32_t (&w)[N
 template <int NL>
 __device__ __forceinline__ void ld_lvl(const unsigned char *row, uint32_t (&w)[NL]) {
     if (NL == 2)
-        asm volatile("ld.global.v2.u32 {%0,%1}, [%2];" : "=r"(w[0]), "=r"(w[1]) : "l"(row));
+        asm volatile("ld.global.cg.v2.u32 {%0,%1}, [%2];" : "=r"(w[0]), "=r"(w[1]) : "l"(row));
     else
-        asm volatile("ld.global.v4.u32 {%0,%1,%2,%3}, [%4];" : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]) : "l"(row));
+        asm volatile("ld.global.cg.v4.u32 {%0,%1,%2,%3}, [%4];" : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]) : "l"(row));
 }
 
 // Software grid barrier (all CTAs co-resident: cooperative launch).  One
@@ -160,8 +173,16 @@ __device__ __forceinline__ void ld_lvl(const unsigned char *row, uint32_t (&w)[N
 // reset between barriers.  Thread 0 also reads the error and overflow flags
 // once, after every CTA has arrived, and hands the verdict to its CTA through
 // shared memory.  Returns false when any CTA recorded an error or an overflow,
-// in which case the caller returns.  The fences around the wait make every
-// write before the barrier (any CTA) visible to every read after it.
+// in which case the caller returns.  The fence before the arrival and the
+// acquire loads and fence after the wait order every write before the
+// barrier (any CTA) before every read after it.  Data that other SMs rewrite
+// between sweeps (state rows, level lists, the unvisited ring, bc, hub
+// slots) is also always read with L2-coherent loads (.cg), never through a
+// possibly stale L1 line.  A barrier does not hold the other CTAs back
+// afterwards: the first CTA out may already work on the next sweep while the
+// last one still reads the counters of the previous one.  So every value read
+// after a barrier is one the next sweep does not write (the per-sweep counter
+// rings of Ctrl, the level lists, each cleared two sweeps ahead).
 __device__ bool grid_sync(Ctrl *c, unsigned int nblocks, unsigned long long wait_ns) {
     __shared__ int ok;
     __syncthreads();
@@ -169,12 +190,11 @@ __device__ bool grid_sync(Ctrl *c, unsigned int nblocks, unsigned long long wait
         __threadfence();
         const unsigned long long arrived = atomicAdd(&c->bar_arrived, 1ull) + 1ull;
         const unsigned long long target = (arrived + nblocks - 1) / nblocks * nblocks;
-        const volatile unsigned long long *cnt = &c->bar_arrived;
         const volatile int *err = &c->error;
         if (arrived != target) {
             unsigned long long t0 = global_ns();
             unsigned int spins = 0;
-            while (*cnt < target) {
+            while (ld_acquire64(&c->bar_arrived) < target) {
                 if ((++spins & 255u) == 0) {
                     if (*err) break;
                     if (global_ns() - t0 > wait_ns) {
@@ -185,6 +205,8 @@ __device__ bool grid_sync(Ctrl *c, unsigned int nblocks, unsigned long long wait
                 __nanosleep(32);
             }
         }
+        // with the arrival fences of the other CTAs, this fence makes their
+        // writes before the barrier visible to this CTA's reads after it
         __threadfence();
         ok = (*err == 0) && (*reinterpret_cast<volatile int *>(&c->overflow) == 0);
     }
@@ -286,6 +308,7 @@ struct SweepCtx {
     uint32_t lb_next;    // list start of level d+1
     uint32_t next_lvl;   // d + 1 (index into lcnt)
     uint32_t split;      // warps per tile (push sweeps over short lists)
+    unsigned long long ubase;  // ring position of this sweep's first unvisited-tile append
 };
 
 __device__ __forceinline__ uint32_t tile_key(uint32_t b, uint32_t level) {
@@ -326,13 +349,15 @@ __device__ __forceinline__ void flush_level(const BatchArgs &a, WarpSmem<S> &ws,
     __syncwarp();
 }
 
-// Writes the warp's buffered unvisited-tile appends to the ring.
+// Writes the warp's buffered unvisited-tile appends to the ring: the sweep's
+// appends occupy ring positions x.ubase, x.ubase + 1, ... (its counter
+// uadd[d % 4] hands them out).
 template <int S>
-__device__ __forceinline__ void flush_unvisited(const BatchArgs &a, WarpSmem<S> &ws, uint32_t cnt) {
+__device__ __forceinline__ void flush_unvisited(const BatchArgs &a, WarpSmem<S> &ws, uint32_t cnt, const SweepCtx &x) {
     const unsigned lane = threadIdx.x & 31;
     unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(&a.ctrl->uctr, (unsigned long long)cnt);
-    base = __shfl_sync(0xffffffffu, base, 0);
+    if (lane == 0) base = atomicAdd(&a.ctrl->uadd[x.d & 3], (unsigned long long)cnt);
+    base = __shfl_sync(0xffffffffu, base, 0) + x.ubase;
     const unsigned long long ring = 2ull * a.ntiles;
     for (uint32_t i = lane; i < cnt; i += 32) a.ulist[(base + i) % ring] = ws.uapp[i];
     __syncwarp();
@@ -371,12 +396,12 @@ __device__ __forceinline__ void append_level(const BatchArgs &a, WarpSmem<S> &ws
 // Appends tile t (kNoTile: nothing; kHubFlag: all chunks) to the ring of tiles
 // that still hold unvisited vertices.  All 32 lanes call it together.
 template <int S>
-__device__ __forceinline__ void append_unvisited(const BatchArgs &a, WarpSmem<S> &ws, uint32_t t) {
+__device__ __forceinline__ void append_unvisited(const BatchArgs &a, WarpSmem<S> &ws, uint32_t t, const SweepCtx &x) {
     const unsigned lane = threadIdx.x & 31;
     if (t != kNoTile && (t & kHubFlag)) {
         const uint32_t t0 = t & ~kHubFlag;
         const uint32_t nch = a.tiles[t0].nchunks;
-        const unsigned long long base = atomicAdd(&a.ctrl->uctr, (unsigned long long)nch);
+        const unsigned long long base = x.ubase + atomicAdd(&a.ctrl->uadd[x.d & 3], (unsigned long long)nch);
         const unsigned long long ring = 2ull * a.ntiles;
         for (uint32_t c = 0; c < nch; ++c) a.ulist[(base + c) % ring] = t0 + c;
         t = kNoTile;
@@ -388,7 +413,7 @@ __device__ __forceinline__ void append_unvisited(const BatchArgs &a, WarpSmem<S>
     cnt += __popc(want);
     __syncwarp();
     if (cnt >= 32) {
-        flush_unvisited<S>(a, ws, cnt);
+        flush_unvisited<S>(a, ws, cnt, x);
         cnt = 0;
     }
     if (lane == 0) ws.nuapp = cnt;
@@ -721,11 +746,14 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
     // that arrives last adds the slots in chunk order and finishes the vertex
     if (hub) {
         unsigned long long *slot0 = a.hub_acc + (size_t)(T.hslot - T.hchunk) * S;
-        if (lane < (unsigned)S) __stcg(slot0 + (size_t)T.hchunk * S + lane, ws.acc[0][lane]);
-        __threadfence();
-        __syncwarp();
         uint32_t last = 0;
-        if (lane == 0) last = (atomicAdd(a.hub_cnt + T.hub, 1u) == T.nchunks - 1);
+        if (lane == 0) {
+            // one thread stores the chunk's slot, fences and arrives (a release)
+#pragma unroll
+            for (int k = 0; k < S; ++k) __stcg(slot0 + (size_t)T.hchunk * S + k, ws.acc[0][k]);
+            __threadfence();
+            last = (atomicAdd(a.hub_cnt + T.hub, 1u) == T.nchunks - 1);
+        }
         last = __shfl_sync(0xffffffffu, last, 0);
         if (!last) return;
         __threadfence();
@@ -788,7 +816,10 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
                 }
                 if (a.dbg_delta) a.dbg_delta[(size_t)k * a.n + v] = delta;
             }
-            if (d > 0 && !a.slot_delta) a.bc[a.ext ? a.ext[v] : v] += add;
+            if (d > 0 && !a.slot_delta) {
+                double *bp = a.bc + (a.ext ? a.ext[v] : v);
+                __stcg(bp, __ldcg(bp) + add);
+            }
         }
     }
     if (MODE == kFwdPull) {
@@ -799,7 +830,7 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
         const bool any = __any_sync(0xffffffffu, nd > 0);
         append_level<S>(a, ws, (any && lane == 0) ? me : kNoTile, x);
         const bool keep = __any_sync(0xffffffffu, left > 0);
-        append_unvisited<S>(a, ws, (keep && lane == 0) ? me : kNoTile);
+        append_unvisited<S>(a, ws, (keep && lane == 0) ? me : kNoTile, x);
     }
 }
 
@@ -877,7 +908,7 @@ __device__ __forceinline__ void run_sweep(const BatchArgs &a, Smem<S> &sm, const
     const uint32_t nitems = nwork * x.split;
     auto item_tile = [&](uint32_t it) -> uint32_t {
         const uint32_t i = it / x.split;
-        if (list) return list[(start + i) % ring];
+        if (list) return __ldcg(list + (start + i) % ring);
         if (!ranges) return i;
         uint32_t lo = 0, hi = nranges;
         while (hi - lo > 1) {
@@ -946,7 +977,7 @@ __device__ __forceinline__ void run_sweep(const BatchArgs &a, Smem<S> &sm, const
         const uint32_t cnt = ws.napp;
         if (cnt) flush_level<S>(a, ws, cnt, x);
         const uint32_t ucnt = ws.nuapp;
-        if (ucnt) flush_unvisited<S>(a, ws, ucnt);
+        if (ucnt) flush_unvisited<S>(a, ws, ucnt, x);
         // per-warp discovery totals into the CTA's counters
         if ((threadIdx.x & 31) == 0 && ws.cnt[0]) {
             atomicAdd(&sm.c_disc, ws.cnt[0]);
@@ -1006,7 +1037,7 @@ __global__ void __launch_bounds__(SweepGeom<S>::kThreads, 1) bc_sweep_kernel(Bat
             pu_cur = (unsigned long long)valid * a.nnz - pf_cur;
         }
         if (blockIdx.x == 0 && threadIdx.x == 0) {
-            for (int s = 0; s < 4; ++s) { c->disc[s] = 0; c->pf[s] = 0; }
+            for (int s = 0; s < 4; ++s) { c->disc[s] = 0; c->pf[s] = 0; c->uadd[s] = 0; }
             for (int k = 0; k < 8; ++k) { c->visited[k] = 0; c->wsum[k] = 0; c->mc2[k] = 0; }
             a.lbase[0] = 0;
             a.lcnt[1] = 0;
@@ -1021,7 +1052,7 @@ __global__ void __launch_bounds__(SweepGeom<S>::kThreads, 1) bc_sweep_kernel(Bat
                 c->mc2[k] = (unsigned long long)ri.x + 2ull * ri.y;
                 const uint32_t tf = a.tile_of[r];
                 const uint32_t t = tf & ~kHubFlag;
-                if (a.tmark[t] == key0) continue;
+                if (vload32(a.tmark + t) == key0) continue;
                 a.tmark[t] = key0;
                 const uint32_t nch = (tf & kHubFlag) ? a.tiles[t].nchunks : 1u;
                 for (uint32_t q = 0; q < nch; ++q) a.lists[n0++] = t + q;
@@ -1096,10 +1127,11 @@ __global__ void __launch_bounds__(SweepGeom<S>::kThreads, 1) bc_sweep_kernel(Bat
         bool uall = true;              // no pull sweep yet: every tile may hold unvisited vertices
         unsigned long long ustart = 0; // ring position / length of the unvisited-tile list
         uint32_t ulen = 0;
-        // ring write position; only pull sweeps move it, so it is read only
-        // right after a barrier (here: after the init barrier), never at the
-        // start of a sweep where a faster CTA may already have appended
-        unsigned long long ucur = vload64(&c->uctr);
+        // ring position of the next pull's appends: every CTA advances it by
+        // the appends of each pull sweep, read from that sweep's own counter
+        // after its barrier (a shared write position would race with CTAs
+        // that already append in the next sweep)
+        unsigned long long ucur = 0;
         // level d's list: loaded together with the sweep counters right after
         // each barrier (one round trip per sweep)
         uint32_t lb = vload32(a.lbase), lc = vload32(a.lcnt);
@@ -1114,6 +1146,7 @@ __global__ void __launch_bounds__(SweepGeom<S>::kThreads, 1) bc_sweep_kernel(Bat
             x.next_lvl = d + 1;
             x.key_next = tile_key(b, d + 1);
             x.split = (x.mode == kFwdPush && lc * 2 < total_warps) ? kPushSplit : 1;
+            x.ubase = ucur;
             if (threadIdx.x == 0) {
                 sm.next = 0;
                 sm.c_disc = 0; sm.c_pf = 0;
@@ -1124,6 +1157,7 @@ __global__ void __launch_bounds__(SweepGeom<S>::kThreads, 1) bc_sweep_kernel(Bat
                     a.lcnt[d + 2] = 0;
                     c->disc[(d + 2) & 3] = 0;
                     c->pf[(d + 2) & 3] = 0;
+                    c->uadd[(d + 2) & 3] = 0;
                 }
             }
             __syncthreads();
@@ -1155,14 +1189,14 @@ __global__ void __launch_bounds__(SweepGeom<S>::kThreads, 1) bc_sweep_kernel(Bat
             if (!grid_sync(c, nblk, wait_ns)) return;
             const unsigned long long disc = vload64(&c->disc[d & 3]);
             const unsigned long long pfn = vload64(&c->pf[d & 3]);
-            const unsigned long long uafter = vload64(&c->uctr);
+            const unsigned long long uadded = vload64(&c->uadd[d & 3]);
             lb = vload32(a.lbase + d + 1);
             lc = vload32(a.lcnt + d + 1);
             trace(a, b, x.mode == kFwdPull ? 2u : 1u, d, walked, disc);
             if (x.mode == kFwdPull) {
                 ustart = ucur;
-                ulen = (uint32_t)(uafter - ucur);
-                ucur = uafter;
+                ulen = (uint32_t)uadded;
+                ucur += uadded;
                 uall = false;
             }
             if (disc == 0) break;
@@ -1184,9 +1218,9 @@ __global__ void __launch_bounds__(SweepGeom<S>::kThreads, 1) bc_sweep_kernel(Bat
                 unsigned char *row = a.rows + v * R;
 #pragma unroll
                 for (int k = 0; k < S; ++k) {
-                    const uint16_t L = *lvl_at(row, k);
+                    const uint16_t L = __ldcg(lvl_at(row, k));
                     if (a.dbg_level) a.dbg_level[(size_t)k * a.n + v] = (L == kUnvisited) ? -1 : (int32_t)L;
-                    if (a.dbg_sigma) a.dbg_sigma[(size_t)k * a.n + v] = (L == kUnvisited) ? 0ull : *val_at<S>(row, k);
+                    if (a.dbg_sigma) a.dbg_sigma[(size_t)k * a.n + v] = (L == kUnvisited) ? 0ull : __ldcg(val_at<S>(row, k));
                 }
             }
             if (!grid_sync(c, nblk, wait_ns)) return;
@@ -1235,9 +1269,10 @@ __global__ void __launch_bounds__(SweepGeom<S>::kThreads, 1) bc_sweep_kernel(Bat
                     const unsigned char *row = a.rows + v * R;
 #pragma unroll
                     for (int k = 0; k < S; ++k) {
-                        const uint16_t L = *reinterpret_cast<const uint16_t *>(row + 2 * k);
+                        const uint16_t L = __ldcg(reinterpret_cast<const unsigned short *>(row) + k);
                         if (L == kUnvisited || L == 0 || !o.out[k]) continue;
-                        o.out[k][v - o.base] += a.slot_delta[(size_t)k * a.n + v];
+                        double *op = o.out[k] + (v - o.base);
+                        __stcg(op, __ldcg(op) + __ldcg(a.slot_delta + (size_t)k * a.n + v));
                     }
                 }
             }
@@ -1252,7 +1287,10 @@ __global__ void __launch_bounds__(SweepGeom<S>::kThreads, 1) bc_sweep_kernel(Bat
                 const size_t idx = (size_t)b * S + k;
                 const unsigned long long W = vload64(&c->wsum[k]);
                 const uint32_t p = packed ? 0u : a.pend[idx];
-                if (p && W >= 2) a.bc[a.ext ? a.ext[r] : r] += (double)p * (double)(W - 2);
+                if (p && W >= 2) {
+                    double *bp = a.bc + (a.ext ? a.ext[r] : r);
+                    __stcg(bp, __ldcg(bp) + (double)p * (double)(W - 2));
+                }
                 a.rstat[idx].visited = vload64(&c->visited[k]);
                 a.rstat[idx].wsum = W;
                 a.rstat[idx].mc2 = vload64(&c->mc2[k]);

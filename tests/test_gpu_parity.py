@@ -224,3 +224,30 @@ def test_rmat12_all_sources_full():
         olvl, osig, odl, _ = oracle.single_source(offs, adj, s)
         assert np.array_equal(lvl, olvl) and np.array_equal(sig, osig)
         assert_bc_close(dl, odl, f"rmat12 delta s={s}")
+
+
+@pytest.mark.parametrize("ratio", ["0", "1e30"])
+def test_every_sweep_pulls_or_pushes(graphs, ratio, monkeypatch):
+    """Forward sweeps forced to one kind (ratio 0: every sweep pulls, 1e30:
+    every sweep pushes) on the pendant graph, whose deep levels have frontiers
+    of a few tiles: a pull there walks about one tile of the unvisited ring
+    per CTA, so CTAs leave its barrier far apart.  The ring window of each
+    pull must be the same in every CTA (a tile walked twice doubles sigma
+    below it, a tile skipped leaves vertices undiscovered)."""
+    monkeypatch.setenv("BCG_PUSH_PULL_RATIO", ratio)
+    offs, adj = graphs["rmat11_pend"]
+    deg = np.diff(offs)
+    with bcg.Graph(offs, adj) as G:
+        for s in [int(v) for v in np.nonzero(deg)[0][:60]]:
+            lvl, sig, dl = G.single_source(s)
+            olvl, osig, odl, _ = oracle.single_source(offs, adj, s)
+            assert np.array_equal(lvl, olvl), (ratio, s)
+            assert np.array_equal(sig, osig), (ratio, s)
+            assert_bc_close(dl, odl, f"ratio={ratio} delta s={s}")
+    src = bcg.sample_sources(len(offs) - 1, 37, 5)
+    ref, _ = oracle.bc(offs, adj, src)
+    for width in (1, 3, 6):
+        with bcg.Graph(offs, adj) as G:
+            G.set_batch_width(width)
+            G.run(src)
+            assert_bc_close(G.bc(), ref, f"ratio={ratio} width={width}")
