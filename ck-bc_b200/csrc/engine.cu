@@ -31,6 +31,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <unordered_map>
 #include <vector>
 
@@ -178,6 +179,39 @@ using namespace bcg;
 
 namespace bcg {
 
+namespace {
+std::mutex g_pool_mu;
+std::vector<cudaMemPool_t> g_pools;  // per device, created on first use
+}  // namespace
+
+cudaError_t tmp_alloc(void **p, size_t bytes, cudaStream_t st) {
+    *p = nullptr;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    cudaMemPool_t pool = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        if (g_pools.size() <= (size_t)dev) g_pools.resize((size_t)dev + 1, nullptr);
+        if (!g_pools[dev]) {
+            cudaMemPoolProps props{};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            if ((e = cudaMemPoolCreate(&g_pools[dev], &props)) != cudaSuccess) {
+                g_pools[dev] = nullptr;
+                return e;
+            }
+            uint64_t keep = 1ull << 30;
+            cudaMemPoolSetAttribute(g_pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        pool = g_pools[dev];
+    }
+    return cudaMallocFromPoolAsync(p, std::max<size_t>(bytes, 16), pool, st);
+}
+
+cudaError_t tmp_free(void *p, cudaStream_t st) { return p ? cudaFreeAsync(p, st) : cudaSuccess; }
+
 static void graph_free(bcg_graph *g) {
     if (!g) return;
     int cur = -1;
@@ -271,7 +305,9 @@ static int setup_tiles(bcg_graph *g, const uint32_t *h_offs) {
     return BCG_OK;
 }
 
-static int create_common(bcg_graph *g, const uint32_t *h_offs) {
+// h_offs: offsets of the searched graph (tiles); h_offs_in: of the input
+// graph (the degree-0 source skip test).
+static int create_common(bcg_graph *g, const uint32_t *h_offs, const uint32_t *h_offs_in) {
     const uint32_t n = g->n;
     // 4 entries of tail padding (the sweep copies 16-byte aligned ranges)
     CK(cudaMalloc(&g->d_vinfo, ((size_t)n + 4) * sizeof(uint2)));
@@ -282,7 +318,9 @@ static int create_common(bcg_graph *g, const uint32_t *h_offs) {
     CK(cudaEventCreate(&g->ev0));
     CK(cudaEventCreate(&g->ev1));
     g->h_deg.resize(n);
-    for (uint32_t v = 0; v < n; ++v) g->h_deg[v] = h_offs[v + 1] - h_offs[v];
+    uint32_t *hd = g->h_deg.data();
+#pragma omp parallel for schedule(static)
+    for (int64_t v = 0; v < (int64_t)n; ++v) hd[v] = h_offs_in[v + 1] - h_offs_in[v];
     const bool prune = (g->flags & BCG_PRUNE_DEGREE1) && !(g->flags & BCG_DIRECTED);
     const unsigned nb = (n + 255) / 256;
     if (prune) {
@@ -366,13 +404,8 @@ struct RunPlan {
 
 // Trees mode: the closed-form bc of the tree vertices (and the anchors' tree
 // terms) for this run's sources, added on the device after the search.
-static int add_tree_terms(bcg_graph *g, const uint32_t *src, uint64_t nsrc, const RunPlan &p, cudaStream_t st,
-                          bcg_stats *stats) {
-    std::vector<uint32_t> s;
-    s.reserve(nsrc);
-    for (uint64_t i = 0; i < nsrc; ++i)
-        if (g->h_deg[src[i]]) s.push_back(src[i]);
-    const int rc = tree_terms(g, s, st);
+static int add_tree_terms(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *stats) {
+    const int rc = tree_terms(g, st);
     if (rc) return rc;
     if (stats) {
         stats->teps_edges += p.tree_edges;
@@ -381,28 +414,45 @@ static int add_tree_terms(bcg_graph *g, const uint32_t *src, uint64_t nsrc, cons
     return BCG_OK;
 }
 
-static int plan_run(const bcg_graph *g, const uint32_t *src, uint64_t nsrc, RunPlan &p) {
+// Trees mode reads each source's anchor words from the device first
+// (tree_source_info on stream st), which also leaves the sources there for
+// the tree terms.
+static int plan_run(bcg_graph *g, const uint32_t *src, uint64_t nsrc, RunPlan &p, cudaStream_t st) {
+    for (uint64_t i = 0; i < nsrc; ++i)
+        if (src[i] >= g->n) return set_error(BCG_ERR_ARG, "source %u >= n=%u", src[i], g->n);
+    std::vector<uint4> info;
+    if (g->trees) {
+        const int rc = tree_source_info(g, src, nsrc, info, st);
+        if (rc) return rc;
+    }
     std::unordered_map<uint32_t, uint32_t> idx;
     idx.reserve(nsrc * 2 + 1);
     for (uint64_t i = 0; i < nsrc; ++i) {
         const uint32_t s = src[i];
-        if (s >= g->n) return set_error(BCG_ERR_ARG, "source %u >= n=%u", s, g->n);
         if (g->h_deg[s] == 0) { ++p.skipped; continue; }
-        const uint32_t r = g->h_anchor.empty() ? s : g->h_anchor[s];
-        if (g->trees && g->h_cdeg[r] == 0) {
-            // a tree component: no kept edges, its bc is all in the tree terms
-            // (the kept vertex r is the last one of its tree: sz[r] is the component)
-            ++p.tree_only;
-            p.tree_edges += g->h_sz[r] - 1;
-            p.tree_verts += g->h_sz[r];
-            continue;
+        uint32_t r = s, root = s;
+        if (g->trees) {
+            const uint4 w = info[i];  // {anchor, its kept degree, internal id, tree size}
+            if (w.y == 0) {
+                // a tree component: no kept edges, its bc is all in the tree
+                // terms (the kept vertex is the last one of its tree: its
+                // tree size is the component)
+                ++p.tree_only;
+                p.tree_edges += w.w - 1;
+                p.tree_verts += w.w;
+                continue;
+            }
+            r = w.x;
+            root = w.z;
+        } else if (!g->h_anchor.empty()) {
+            r = root = g->h_anchor[s];
         }
         auto it = idx.find(r);
         uint32_t k;
         if (it == idx.end()) {
             k = (uint32_t)p.roots.size();
             idx.emplace(r, k);
-            p.roots.push_back(g->h_intl.empty() ? r : g->h_intl[r]);
+            p.roots.push_back(root);
             p.pend.push_back(0);
             p.mult.push_back(0.0);
             p.count.push_back(0);
@@ -697,10 +747,10 @@ static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint3
         // the input CSR on the device (a temporary copy for host input)
         const uint32_t *d_offs0 = offsets, *d_adj0 = adj;
         uint32_t *t_offs = nullptr, *t_adj = nullptr;
-        auto drop = [&]() { cudaFree(t_offs); cudaFree(t_adj); };
+        auto drop = [&]() { tmp_free(t_offs, 0); tmp_free(t_adj, 0); };
         if (!device_in) {
-            if ((e = cudaMalloc(&t_offs, ((size_t)n + 1) * sizeof(uint32_t))) != cudaSuccess ||
-                (e = cudaMalloc(&t_adj, std::max<uint64_t>(nnz, 1) * sizeof(uint32_t))) != cudaSuccess ||
+            if ((e = tmp_alloc(&t_offs, ((size_t)n + 1) * sizeof(uint32_t), 0)) != cudaSuccess ||
+                (e = tmp_alloc(&t_adj, std::max<uint64_t>(nnz, 1) * sizeof(uint32_t), 0)) != cudaSuccess ||
                 (e = cudaMemcpy(t_offs, offsets, ((size_t)n + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice)) !=
                     cudaSuccess ||
                 (nnz && (e = cudaMemcpy(t_adj, adj, nnz * sizeof(uint32_t), cudaMemcpyHostToDevice)) != cudaSuccess)) {
@@ -729,19 +779,16 @@ static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint3
             (e = cudaMemset(g->d_adj + nnz, 0, 4 * sizeof(uint32_t))) != cudaSuccess)
             return fail(set_error(BCG_ERR_CUDA, "uploading CSR: %s", cudaGetErrorString(e)));
     }
-    rc = create_common(g, trees ? h_offs2.data() : ho);
+    rc = create_common(g, trees ? h_offs2.data() : ho, ho);
     if (rc) return fail(rc);
     if (trees) {
-        // kept-graph degrees and tree weights (reach) for the searches, input
-        // degrees for the source skip test
+        // kept-graph degrees and tree weights (reach) for the searches
         g->trees = true;
         g->nnz = nnz;
-        for (uint32_t v = 0; v < n; ++v) g->h_deg[v] = ho[v + 1] - ho[v];
         if ((e = cudaMemcpy(g->d_vinfo, g->d_vinfo_trees, (size_t)n * sizeof(uint2), cudaMemcpyDeviceToDevice)) !=
             cudaSuccess)
             return fail(set_error(BCG_ERR_CUDA, "tree weights: %s", cudaGetErrorString(e)));
         cudaFree(g->d_vinfo_trees);
-    cudaFree(g->d_level_out);
         g->d_vinfo_trees = nullptr;
     }
     *out = g;
@@ -780,11 +827,11 @@ int bcg_run(bcg_graph *g, const uint32_t *sources, uint64_t nsrc, bcg_stats *sta
     *st = bcg_stats{};
     st->sources = nsrc;
     RunPlan p;
-    int rc = plan_run(g, sources, nsrc, p);
+    int rc = plan_run(g, sources, nsrc, p, 0);
     if (rc) return rc;
     rc = run_plan(g, p, 0, st, DebugOut{});
     if (rc || !g->trees) return rc;
-    return add_tree_terms(g, sources, nsrc, p, 0, st);
+    return add_tree_terms(g, p, 0, st);
 }
 
 int bcg_run_device(bcg_graph *g, const uint32_t *d_sources, uint64_t nsrc, void *stream, bcg_stats *stats) {
@@ -798,11 +845,11 @@ int bcg_run_device(bcg_graph *g, const uint32_t *d_sources, uint64_t nsrc, void 
     }
     if (stats) { *stats = bcg_stats{}; stats->sources = nsrc; }
     RunPlan p;
-    int rc = plan_run(g, h.data(), nsrc, p);
+    int rc = plan_run(g, h.data(), nsrc, p, st);
     if (rc) return rc;
     rc = run_plan(g, p, st, stats, DebugOut{});
     if (rc || !g->trees) return rc;
-    return add_tree_terms(g, h.data(), nsrc, p, st, stats);
+    return add_tree_terms(g, p, st, stats);
 }
 
 int bcg_get_bc(bcg_graph *g, double *bc_host) {
@@ -846,11 +893,20 @@ static int debug_batch_impl(bcg_graph *g, uint32_t width, const uint32_t *roots,
     const size_t n = g->n;
     const size_t ns = g->tile_n ? g->tile_n : g->n;  // searched vertices (the kernel's stride)
     RunPlan p;
+    for (uint32_t k = 0; k < nroots; ++k)
+        if (roots[k] >= g->n) return set_error(BCG_ERR_ARG, "root %u >= n=%u", roots[k], g->n);
+    std::vector<uint4> info;
+    std::vector<uint32_t> intl;  // trees mode: caller's id -> internal id
+    if (g->trees) {
+        int rc = tree_source_info(g, roots, nroots, info, 0);
+        if (rc) return rc;
+        intl.resize(n);
+        CK(cudaMemcpy(intl.data(), g->tdev.intl, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    }
     for (uint32_t k = 0; k < nroots; ++k) {
         const uint32_t r = roots[k];
-        if (r >= g->n) return set_error(BCG_ERR_ARG, "root %u >= n=%u", r, g->n);
-        const uint32_t ri = g->h_intl.empty() ? r : g->h_intl[r];
-        if (g->trees && (g->h_cdeg[r] == 0 || ri >= ns))
+        const uint32_t ri = g->trees ? info[k].z : r;
+        if (g->trees && (info[k].x != r || info[k].y == 0 || ri >= ns))
             return set_error(BCG_ERR_ARG, "root %u is not searched: it lies in a pendant tree or has no kept edge", r);
         p.roots.push_back(ri);
         p.pend.push_back(0);
@@ -899,7 +955,7 @@ static int debug_batch_impl(bcg_graph *g, uint32_t width, const uint32_t *roots,
     if (rc) return rc;
     for (uint32_t k = 0; k < nroots; ++k) {
         for (size_t v = 0; v < n; ++v) {
-            const size_t vi = g->h_intl.empty() ? v : g->h_intl[v];
+            const size_t vi = g->trees ? intl[v] : v;
             const bool held = vi < ns;
             const int32_t L = held ? hl[k * ns + vi] : -1;
             if (level) level[k * n + v] = L;
@@ -960,7 +1016,8 @@ int bcg_graph_pruning(bcg_graph *g, uint32_t *anchor, uint32_t *reach) {
     if (!g) return set_error(BCG_ERR_ARG, "null handle");
     const size_t n = g->n;
     if (anchor) {
-        if (g->h_anchor.empty()) for (size_t v = 0; v < n; ++v) anchor[v] = (uint32_t)v;
+        if (g->trees) CK(cudaMemcpy(anchor, g->tdev.anchor, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        else if (g->h_anchor.empty()) for (size_t v = 0; v < n; ++v) anchor[v] = (uint32_t)v;
         else memcpy(anchor, g->h_anchor.data(), n * sizeof(uint32_t));
     }
     if (reach) {

@@ -24,11 +24,17 @@ struct TreeDev {
     uint32_t *comp = nullptr;    // component of the input graph (a root's internal id)
     unsigned long long *comp_n = nullptr;  // vertices per component, indexed by root
     uint32_t *order = nullptr;   // peeled vertices, round by round
+    uint32_t *anchor = nullptr;  // kept vertex a peeled vertex's tree hangs from (itself when kept)
+    uint32_t *intl = nullptr;    // caller's id -> internal id of the searched graph
+    uint32_t *cdeg = nullptr;    // degree in the kept graph
     std::vector<uint32_t> round_off;  // start of each round in order, and the end
     uint32_t npeeled = 0;
-    // per-run scratch of the closed-form tree terms
+    // per-run scratch: the run's sources (uploaded by tree_source_info), their
+    // planning words, and the closed-form tree terms
     uint32_t *cnt = nullptr, *src = nullptr;
+    uint4 *info = nullptr;
     size_t src_cap = 0;
+    uint64_t nsrc = 0;
     unsigned long long *sub = nullptr, *csrc = nullptr, *acc = nullptr;
 };
 }  // namespace bcg
@@ -66,16 +72,13 @@ struct bcg_graph {
     float ratio = 0.2f;
     bool trees = false;               // BCG_PRUNE_TREES: pendant trees folded (tdev)
     bcg::TreeDev tdev;
-    std::vector<uint32_t> h_cdeg;     // degrees in the kept graph, caller's numbering (trees mode)
-    std::vector<uint32_t> h_sz;       // subtree sizes, caller's numbering (trees mode)
     uint2 *d_vinfo_trees = nullptr;   // degree/reach words built by the peeling (until creation ends)
     int32_t *d_level_out = nullptr;   // depths exported by bcg_run_root_levels
     // Trees mode numbers the searched vertices internally: the vertices with
     // kept edges first (caller's order), then the rest, so the tiles cover
-    // [0, tile_n) only.  h_intl: caller's id -> internal id; d_ext: internal
-    // id -> caller's id, where the sweep adds each vertex's bc.
+    // [0, tile_n) only.  tdev.intl: caller's id -> internal id; d_ext:
+    // internal id -> caller's id, where the sweep adds each vertex's bc.
     uint32_t tile_n = 0;              // vertices covered by tiles (0: all n)
-    std::vector<uint32_t> h_intl;     // empty: internal ids are the caller's
     uint32_t *d_ext = nullptr;
     int sigma_mode = 0;               // 0 auto (exact, extended on overflow), 1 exact only, 2 extended
     double *d_bc_save = nullptr;      // accumulators before an automatic-mode run
@@ -84,6 +87,17 @@ struct bcg_graph {
 };
 
 namespace bcg {
+
+// Temporaries of graph creation, from a library-owned stream-ordered pool of
+// the current device that keeps up to 1 GiB reserved once they are freed:
+// creating graphs one after another then neither maps fresh memory nor
+// waits for the device in cudaFree.  Ordered on stream st like a kernel.
+cudaError_t tmp_alloc(void **p, size_t bytes, cudaStream_t st);
+cudaError_t tmp_free(void *p, cudaStream_t st);
+template <class T>
+cudaError_t tmp_alloc(T **p, size_t bytes, cudaStream_t st) {
+    return tmp_alloc(reinterpret_cast<void **>(p), bytes, st);
+}
 
 // ext: sigma and X as extended-range numbers (ext64.cuh) instead of uint64 / double
 int launch_sweep(int S, const BatchArgs &a, cudaStream_t st, int *grid_out, bool ext = false);
@@ -113,14 +127,18 @@ int graph_retile(bcg_graph *g, uint32_t vcap, uint32_t ecap, bool force = false)
 // Peels the pendant trees of the input CSR (device arrays d_offs0 / d_adj0,
 // nnz entries; check_ids: verify every id < n first) and builds g's kept
 // graph in internal numbering (d_offs, d_adj, d_ext, tile_n, degree/reach
-// words in d_vinfo_trees), the tree arrays (tdev) and the host lookups
-// (h_anchor, h_cdeg, h_intl, h_sz).  h_offs2: the kept graph's offsets.
+// words in d_vinfo_trees) and the tree arrays (tdev).  h_offs2: the kept
+// graph's offsets.
 int prepare_trees(bcg_graph *g, const uint32_t *d_offs0, const uint32_t *d_adj0, uint64_t nnz, bool check_ids,
                   std::vector<uint32_t> &h_offs2);
+// Uploads the k sources src (caller's ids, all < n) and reads back, per
+// source s, {anchor a of s, kept degree of a, internal id of a, tree size of
+// a}; the sources stay on the device for tree_terms.  Synchronises st.
+int tree_source_info(bcg_graph *g, const uint32_t *src, uint64_t k, std::vector<uint4> &info, cudaStream_t st);
 // Adds the closed-form betweenness of the tree vertices (and the anchors'
-// tree terms) for the sources src (degree > 0, caller's ids, duplicates
-// count) into g's bc, on stream st.
-int tree_terms(bcg_graph *g, const std::vector<uint32_t> &src, cudaStream_t st);
+// tree terms) for the sources of the last tree_source_info call (duplicates
+// count; sources of degree 0 add nothing) into g's bc, on stream st.
+int tree_terms(bcg_graph *g, cudaStream_t st);
 void tree_free(bcg_graph *g);
 // Uploads ngraphs host CSR graphs as one disjoint union (graph order[p] at
 // union position p, its vertex v at base[order[p]] + v; with by_active the

@@ -34,9 +34,9 @@
 // The kept graph is renumbered so that the vertices that keep an edge come
 // first (in their original order), by a device scan; its lists stay sorted.
 // Components (for n_comp) are labelled by a union-find over the kept graph
-// (roots hooked smaller-under-larger, so every component's root is its
-// smallest internal id) and extended to the tree vertices through their
-// anchors.
+// (larger roots hooked under smaller ones, so every component's root is its
+// smallest internal id; links in the Afforest order, k_uf_link_nth) and
+// extended to the tree vertices through their anchors.
 #include <algorithm>
 #include <vector>
 
@@ -101,7 +101,7 @@ int scan_exclusive(const uint32_t *d_in, uint32_t *d_out, uint64_t len, cudaStre
     if (len == 0) return BCG_OK;
     const uint64_t nb = (len + kScanBlock - 1) / kScanBlock;
     uint32_t *bsum = nullptr;
-    CKT(cudaMalloc(&bsum, nb * sizeof(uint32_t)));
+    CKT(tmp_alloc(&bsum, nb * sizeof(uint32_t), st));
     k_scan_block<<<(unsigned)nb, kScanBlock, 0, st>>>(d_in, d_out, bsum, len);
     int rc = BCG_OK;
     if (cudaGetLastError() != cudaSuccess) rc = set_error(BCG_ERR_CUDA, "scan launch failed");
@@ -112,8 +112,7 @@ int scan_exclusive(const uint32_t *d_in, uint32_t *d_out, uint64_t len, cudaStre
             if (cudaGetLastError() != cudaSuccess) rc = set_error(BCG_ERR_CUDA, "scan launch failed");
         }
     }
-    cudaStreamSynchronize(st);
-    cudaFree(bsum);
+    tmp_free(bsum, st);
     return rc;
 }
 
@@ -272,25 +271,53 @@ __global__ void k_uf_init(uint32_t n, uint32_t *__restrict__ root) {
     if (v < n) root[v] = v;
 }
 
-// One warp per live vertex hooks it to its larger neighbours.
-__global__ void k_uf_link(uint32_t nlive, const uint32_t *__restrict__ offs2, const uint32_t *__restrict__ adj2,
-                          uint32_t *root) {
+// Joins the sets of v and u: the larger root is hooked under the smaller
+// one by a compare-and-swap (retried from the new roots when another thread
+// hooked it first).
+__device__ __forceinline__ void uf_link(uint32_t *root, uint32_t v, uint32_t u) {
+    uint32_t a = uf_find(root, v), b = uf_find(root, u);
+    while (a != b) {
+        if (a < b) { const uint32_t t = a; a = b; b = t; }  // hook the larger root a under b
+        const uint32_t old = atomicCAS(root + a, a, b);
+        if (old == a) break;
+        a = uf_find(root, old);
+        b = uf_find(root, b);
+    }
+}
+
+// Components in the manner of Afforest (Sutton, Ben-Nun and Barak, IPDPS
+// 2018): every vertex is first linked to its first and its second neighbour
+// only, after which most vertices already share the root of the largest
+// component; then only the vertices outside it link their remaining
+// neighbours.  The lists are symmetric, so an edge with an end outside the
+// largest component is linked from that end, and an edge inside it joins
+// nothing new.
+__global__ void k_uf_link_nth(uint32_t nlive, const uint32_t *__restrict__ offs2, const uint32_t *__restrict__ adj2,
+                              uint32_t *root, uint32_t j) {
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nlive) return;
+    const uint32_t e = offs2[v] + j;
+    if (e < offs2[v + 1]) uf_link(root, v, adj2[e]);
+}
+
+// One warp per live vertex outside the set of root `skip`: links its
+// neighbours from the (from)-th on.  (A vertex whose root was rewritten
+// meanwhile is simply linked in full.)
+__global__ void k_uf_link_rest(uint32_t nlive, const uint32_t *__restrict__ offs2, const uint32_t *__restrict__ adj2,
+                               uint32_t *root, uint32_t from, uint32_t skip) {
     const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const unsigned lane = threadIdx.x & 31;
     if (w >= nlive) return;
     const uint32_t v = (uint32_t)w;
-    for (uint32_t e = offs2[v] + lane; e < offs2[v + 1]; e += 32) {
-        const uint32_t u = adj2[e];
-        if (u <= v) continue;  // each edge once
-        uint32_t a = uf_find(root, v), b = uf_find(root, u);
-        while (a != b) {
-            if (a < b) { const uint32_t t = a; a = b; b = t; }  // hook the larger root a under b
-            const uint32_t old = atomicCAS(root + a, a, b);
-            if (old == a) break;
-            a = uf_find(root, old);
-            b = uf_find(root, b);
-        }
-    }
+    if (reinterpret_cast<volatile uint32_t *>(root)[v] == skip) return;
+    for (uint32_t e = offs2[v] + from + lane; e < offs2[v + 1]; e += 32) uf_link(root, v, adj2[e]);
+}
+
+// root[i * nlive / kSamples] for the sampled vertices.
+constexpr uint32_t kSamples = 1024;
+__global__ void k_uf_sample(uint32_t nlive, const uint32_t *__restrict__ root, uint32_t *__restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < kSamples) out[i] = root[(uint32_t)(((uint64_t)i * nlive) / kSamples)];
 }
 
 // After linking every root is final.  The walk here stores nothing on the
@@ -322,6 +349,17 @@ __global__ void k_tp_comp(uint32_t n, const uint32_t *__restrict__ anchor, const
 __global__ void k_check_ids(uint64_t nnz, uint32_t n, const uint32_t *__restrict__ adj, unsigned long long *bad) {
     for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += (uint64_t)gridDim.x * blockDim.x)
         if (adj[e] >= n) atomicMin(bad, (unsigned long long)e);
+}
+
+// What the run planning needs of each source s (ids checked < n on the
+// host): its anchor a, and a's kept degree, internal id and tree size.
+__global__ void k_src_info(uint64_t k, const uint32_t *__restrict__ src, const uint32_t *__restrict__ anchor,
+                           const uint32_t *__restrict__ cdeg, const uint32_t *__restrict__ intl,
+                           const uint32_t *__restrict__ sz, uint4 *__restrict__ out) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= k) return;
+    const uint32_t a = anchor[src[i]];
+    out[i] = make_uint4(a, cdeg[a], intl[a], sz[a]);
 }
 
 // ---- per-run tree terms
@@ -372,7 +410,8 @@ __global__ void k_tt_add(uint32_t n, const unsigned long long *__restrict__ acc,
 void tree_free(bcg_graph *g) {
     TreeDev &t = g->tdev;
     cudaFree(t.parent); cudaFree(t.sz); cudaFree(t.comp); cudaFree(t.comp_n); cudaFree(t.order);
-    cudaFree(t.cnt); cudaFree(t.sub); cudaFree(t.csrc); cudaFree(t.acc); cudaFree(t.src);
+    cudaFree(t.anchor); cudaFree(t.intl); cudaFree(t.cdeg);
+    cudaFree(t.cnt); cudaFree(t.sub); cudaFree(t.csrc); cudaFree(t.acc); cudaFree(t.src); cudaFree(t.info);
     t = TreeDev{};
 }
 
@@ -381,30 +420,31 @@ int prepare_trees(bcg_graph *g, const uint32_t *d_offs0, const uint32_t *d_adj0,
     const uint32_t n = g->n;
     cudaStream_t st = 0;
     TreeDev &t = g->tdev;
-    uint32_t *deg = nullptr, *rem = nullptr, *anchor = nullptr, *cand = nullptr, *fa = nullptr, *fb = nullptr,
-             *ctr = nullptr, *cdeg = nullptr, *tmp = nullptr, *intl = nullptr, *root = nullptr;
+    uint32_t *deg = nullptr, *rem = nullptr, *cand = nullptr, *fa = nullptr, *fb = nullptr, *ctr = nullptr,
+             *tmp = nullptr, *root = nullptr;
     unsigned long long *bad = nullptr;
     auto cleanup = [&]() {
-        cudaFree(deg); cudaFree(rem); cudaFree(anchor); cudaFree(cand); cudaFree(fa); cudaFree(fb);
-        cudaFree(ctr); cudaFree(cdeg); cudaFree(tmp); cudaFree(intl); cudaFree(root); cudaFree(bad);
+        tmp_free(deg, st); tmp_free(rem, st); tmp_free(cand, st); tmp_free(fa, st); tmp_free(fb, st);
+        tmp_free(ctr, st); tmp_free(tmp, st); tmp_free(root, st); tmp_free(bad, st);
     };
     struct Guard { decltype(cleanup) &f; ~Guard() { f(); } } guard{cleanup};
     const size_t nb = (size_t)n * sizeof(uint32_t);
     if (check_ids && nnz) {
-        CKT(cudaMalloc(&bad, sizeof(unsigned long long)));
+        CKT(tmp_alloc(&bad, sizeof(unsigned long long), st));
         CKT(cudaMemset(bad, 0xFF, sizeof(unsigned long long)));
         k_check_ids<<<148 * 8, 256, 0, st>>>(nnz, n, d_adj0, bad);
         unsigned long long hb = 0;
         CKT(cudaMemcpy(&hb, bad, sizeof(hb), cudaMemcpyDeviceToHost));
         if (hb != ~0ull) return set_error(BCG_ERR_ARG, "adj[%llu] >= n", hb);
     }
-    CKT(cudaMalloc(&deg, nb));
-    CKT(cudaMalloc(&rem, nb));
-    CKT(cudaMalloc(&anchor, nb));
-    CKT(cudaMalloc(&cand, nb));
-    CKT(cudaMalloc(&fa, nb));
-    CKT(cudaMalloc(&fb, nb));
-    CKT(cudaMalloc(&ctr, 4 * sizeof(uint32_t)));
+    CKT(tmp_alloc(&deg, nb, st));
+    CKT(tmp_alloc(&rem, nb, st));
+    CKT(cudaMalloc(&t.anchor, nb));
+    uint32_t *const anchor = t.anchor;
+    CKT(tmp_alloc(&cand, nb, st));
+    CKT(tmp_alloc(&fa, nb, st));
+    CKT(tmp_alloc(&fb, nb, st));
+    CKT(tmp_alloc(&ctr, 4 * sizeof(uint32_t), st));
     CKT(cudaMalloc(&t.parent, nb));
     CKT(cudaMalloc(&t.sz, nb));
     CKT(cudaMalloc(&t.order, nb));
@@ -434,9 +474,10 @@ int prepare_trees(bcg_graph *g, const uint32_t *d_offs0, const uint32_t *d_adj0,
     }
     CKT(cudaGetLastError());
     // the kept graph, renumbered
-    CKT(cudaMalloc(&cdeg, nb));
-    CKT(cudaMalloc(&tmp, nb + 4 * sizeof(uint32_t)));
-    CKT(cudaMalloc(&intl, nb));
+    CKT(cudaMalloc(&t.cdeg, nb));
+    CKT(tmp_alloc(&tmp, nb + 4 * sizeof(uint32_t), st));
+    CKT(cudaMalloc(&t.intl, nb));
+    uint32_t *const cdeg = t.cdeg, *const intl = t.intl;
     CKT(cudaMalloc(&g->d_ext, nb));
     k_tp_cdeg<<<nblocks((uint64_t)n * 32, 256), 256, 0, st>>>(n, d_offs0, d_adj0, rem, cdeg);
     k_tp_flag<<<nblocks(n, 256), 256, 0, st>>>(n, cdeg, tmp);
@@ -467,12 +508,34 @@ int prepare_trees(bcg_graph *g, const uint32_t *d_offs0, const uint32_t *d_adj0,
     CKT(cudaMalloc(&g->d_vinfo_trees, (size_t)n * sizeof(uint2)));
     k_tp_vinfo<<<nblocks(n, 256), 256, 0, st>>>(n, g->d_ext, cdeg, rem, t.sz, g->d_vinfo_trees);
     // components
-    CKT(cudaMalloc(&root, nb));
+    CKT(tmp_alloc(&root, nb, st));
     CKT(cudaMalloc(&t.comp, nb));
     CKT(cudaMalloc(&t.comp_n, (size_t)n * sizeof(unsigned long long)));
     CKT(cudaMemset(t.comp_n, 0, (size_t)n * sizeof(unsigned long long)));
     k_uf_init<<<nblocks(n, 256), 256, 0, st>>>(n, root);
-    if (nlive) k_uf_link<<<nblocks((uint64_t)nlive * 32, 256), 256, 0, st>>>(nlive, g->d_offs, g->d_adj, root);
+    if (nlive) {
+        for (uint32_t j = 0; j < 2; ++j) {
+            k_uf_link_nth<<<nblocks(nlive, 256), 256, 0, st>>>(nlive, g->d_offs, g->d_adj, root, j);
+            k_uf_flatten<<<nblocks(nlive, 256), 256, 0, st>>>(nlive, root);
+        }
+        // the most frequent root among evenly spaced samples
+        uint32_t *d_smp = nullptr;
+        CKT(tmp_alloc(&d_smp, kSamples * sizeof(uint32_t), st));
+        k_uf_sample<<<nblocks(kSamples, 256), 256, 0, st>>>(nlive, root, d_smp);
+        std::vector<uint32_t> smp(kSamples);
+        const cudaError_t ce = cudaMemcpy(smp.data(), d_smp, kSamples * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+        tmp_free(d_smp, st);
+        CKT(ce);
+        std::sort(smp.begin(), smp.end());
+        uint32_t giant = smp[0], best = 0;
+        for (size_t i = 0; i < smp.size();) {
+            size_t j = i;
+            while (j < smp.size() && smp[j] == smp[i]) ++j;
+            if (j - i > best) { best = (uint32_t)(j - i); giant = smp[i]; }
+            i = j;
+        }
+        k_uf_link_rest<<<nblocks((uint64_t)nlive * 32, 256), 256, 0, st>>>(nlive, g->d_offs, g->d_adj, root, 2u, giant);
+    }
     k_uf_flatten<<<nblocks(n, 256), 256, 0, st>>>(n, root);
     k_tp_comp<<<nblocks(n, 256), 256, 0, st>>>(n, anchor, intl, root, t.comp, t.comp_n);
     CKT(cudaGetLastError());
@@ -481,36 +544,44 @@ int prepare_trees(bcg_graph *g, const uint32_t *d_offs0, const uint32_t *d_adj0,
     CKT(cudaMalloc(&t.sub, (size_t)n * sizeof(unsigned long long)));
     CKT(cudaMalloc(&t.csrc, (size_t)n * sizeof(unsigned long long)));
     CKT(cudaMalloc(&t.acc, (size_t)n * sizeof(unsigned long long)));
-    // host copies the source planning needs
-    g->h_anchor.resize(n);
-    g->h_cdeg.resize(n);
-    g->h_intl.resize(n);
-    g->h_sz.resize(n);
-    CKT(cudaMemcpy(g->h_anchor.data(), anchor, nb, cudaMemcpyDeviceToHost));
-    CKT(cudaMemcpy(g->h_cdeg.data(), cdeg, nb, cudaMemcpyDeviceToHost));
-    CKT(cudaMemcpy(g->h_intl.data(), intl, nb, cudaMemcpyDeviceToHost));
-    CKT(cudaMemcpy(g->h_sz.data(), t.sz, nb, cudaMemcpyDeviceToHost));
     g->tile_n = nlive ? nlive : 1;
     g->npruned = t.npeeled;
     return BCG_OK;
 }
 
-int tree_terms(bcg_graph *g, const std::vector<uint32_t> &src, cudaStream_t st) {
+int tree_source_info(bcg_graph *g, const uint32_t *src, uint64_t k, std::vector<uint4> &info, cudaStream_t st) {
+    TreeDev &t = g->tdev;
+    t.nsrc = 0;
+    info.resize(k);
+    if (k == 0) return BCG_OK;
+    if (t.src_cap < k) {
+        cudaFree(t.src);
+        cudaFree(t.info);
+        t.src = nullptr;
+        t.info = nullptr;
+        t.src_cap = 0;
+        CKT(cudaMalloc(&t.src, k * sizeof(uint32_t)));
+        CKT(cudaMalloc(&t.info, k * sizeof(uint4)));
+        t.src_cap = k;
+    }
+    CKT(cudaMemcpyAsync(t.src, src, k * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    k_src_info<<<nblocks(k, 256), 256, 0, st>>>(k, t.src, t.anchor, t.cdeg, t.intl, t.sz, t.info);
+    CKT(cudaGetLastError());
+    CKT(cudaMemcpyAsync(info.data(), t.info, k * sizeof(uint4), cudaMemcpyDeviceToHost, st));
+    CKT(cudaStreamSynchronize(st));
+    t.nsrc = k;
+    return BCG_OK;
+}
+
+int tree_terms(bcg_graph *g, cudaStream_t st) {
     TreeDev &t = g->tdev;
     const uint32_t n = g->n;
-    if (src.empty()) return BCG_OK;
-    if (t.src_cap < src.size()) {
-        cudaFree(t.src);
-        t.src = nullptr;
-        t.src_cap = 0;
-        CKT(cudaMalloc(&t.src, src.size() * sizeof(uint32_t)));
-        t.src_cap = src.size();
-    }
-    CKT(cudaMemcpyAsync(t.src, src.data(), src.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    const uint64_t k = t.nsrc;
+    if (k == 0) return BCG_OK;
     CKT(cudaMemsetAsync(t.cnt, 0, (size_t)n * sizeof(uint32_t), st));
     CKT(cudaMemsetAsync(t.csrc, 0, (size_t)n * sizeof(unsigned long long), st));
     CKT(cudaMemsetAsync(t.acc, 0, (size_t)n * sizeof(unsigned long long), st));
-    k_tt_count<<<nblocks(src.size(), 256), 256, 0, st>>>(src.size(), t.src, t.cnt);
+    k_tt_count<<<nblocks(k, 256), 256, 0, st>>>(k, t.src, t.cnt);
     k_tt_init<<<nblocks(n, 256), 256, 0, st>>>(n, t.cnt, t.comp, t.sub, t.csrc);
     for (size_t r = 0; r + 1 < t.round_off.size(); ++r) {
         const uint32_t o = t.round_off[r], c = t.round_off[r + 1] - o;
