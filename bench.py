@@ -627,8 +627,10 @@ def main():
     clocks = ClockSampler(local)
     clocks.start()
     step_ms, kern_ms, edges, cverts, ran, s_edges, s_verts, roots = [], [], 0, 0, 0, 0, 0, 0
+    launches = 0  # this library's kernels (bcg_stats.launches): the sweep, the source gather, the tree terms
     for _ in range(args.steps):
         ms, st = one_step()
+        launches += st.launches
         step_ms.append(ms)
         kern_ms.append(st.kernel_ms)
         edges += st.teps_edges
@@ -726,7 +728,7 @@ def main():
                           else "1 GPU",
                           "l2": "512 MiB flush write between steps (untimed); graph + state exceed L2"},
                "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clk,
-               "gpu_launches": args.steps}
+               "gpu_launches": int(launches)}
         print(json.dumps(out), flush=True)
     g.close()
     if dist is not None:

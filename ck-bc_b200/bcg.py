@@ -57,7 +57,7 @@ class Stats(ctypes.Structure):
                 ("comp_vertices", ctypes.c_uint64),
                 ("max_depth", ctypes.c_uint32), ("batch_width", ctypes.c_uint32),
                 ("kernel_ms", ctypes.c_double), ("extended_sigma", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
-                ("search_edges", ctypes.c_uint64)]
+                ("search_edges", ctypes.c_uint64), ("launches", ctypes.c_uint64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -108,6 +108,10 @@ SIGNATURES = {
                                         ctypes.POINTER(Stats)]),
     "bcg_run_root_levels": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_double, ctypes.c_uint32,
                                            _i32p, ctypes.POINTER(Stats)]),
+    "bcg_run_slots": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, _u32p, ctypes.c_uint32, ctypes.c_void_p,
+                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "bcg_add_scaled": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_uint32,
+                                      ctypes.c_double]),
     "bcg_set_batch_width": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32]),
     "bcg_set_sigma_mode": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "bcg_single_source_ext": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, _i32p, _u64p, _f64p]),

@@ -20,12 +20,28 @@ namespace {
 
 bcg_graph *g_graph = nullptr;
 std::vector<uint32_t> g_deg;       // degree of every vertex (CSC column lengths)
-std::vector<int32_t> g_level;      // BFS depth of the current source (-1 = not reached)
 std::vector<uint32_t> g_count;     // vertices per level of the current source
 uint32_t g_v0 = 0;
 uint32_t g_reach_v0 = 0;
 bool g_pending = false;            // the current source's search has not run yet
+bool g_committed = true;           // the current source's dependencies are in bc
 uint64_t g_reach_visited = 0;      // sum of reach over the vertices it reached, root excluded
+
+// Sources searched ahead: the driver asks for its sources one at a time, in
+// increasing order, skipping degree 0 (bc2d.c:1016-1036), so the first
+// source of a batch is searched together with the next kAhead - 1 candidates
+// (bcg_run_slots: nothing added to bc).  A source's dependencies are added
+// when the driver commits it (update_bc_cuda); a candidate it never asks
+// for is dropped.
+constexpr uint32_t kAhead = 6;
+struct Ahead {
+    uint32_t nroots = 0;
+    uint32_t roots[kAhead] = {};
+    uint64_t visited[kAhead] = {}, wsum[kAhead] = {};
+    std::vector<int32_t> level;  // kAhead * n depths (-1 = not reached)
+    double *d_delta = nullptr;   // kAhead * n dependencies on the device
+} g_ahead;
+uint32_t g_slot = 0;               // the current source's slot in g_ahead
 
 [[noreturn]] void fail(const char *what, int rc) {
     fprintf(stderr, "bc2d_compat: %s failed (%d): %s\n", what, rc, bcg_last_error());
@@ -42,7 +58,12 @@ size_t initcuda(uint64_t ned, LOCINT *col, LOCINT *row) {
     if (rc) fail("initcuda", rc);
     g_deg.resize(n);
     for (uint32_t v = 0; v < n; ++v) g_deg[v] = col[v + 1] - col[v];
-    g_level.assign(n, -1);
+    g_ahead = Ahead{};
+    g_ahead.level.assign((size_t)kAhead * n, -1);
+    if (cudaMalloc(&g_ahead.d_delta, (size_t)kAhead * n * sizeof(double)) != cudaSuccess) {
+        fprintf(stderr, "bc2d_compat: initcuda: cudaMalloc of %zu bytes failed\n", (size_t)kAhead * n * sizeof(double));
+        exit(EXIT_FAILURE);
+    }
     printf("ROWBL = %i - ROWPP = %i\n", (int)n, (int)n);
     return (size_t)(n + 1) * 4 + ned * 4 + (size_t)n * (8 + 8 + 16);
 }
@@ -62,53 +83,81 @@ void setcuda(uint64_t, LOCINT *, LOCINT *, LOCINT reach_v0) {
 // The driver's per-source sequence (bc_func_mono, bc2d.c:504-580) is
 // setcuda, set_mlp_cuda, then scan_col_csc_cuda_mono per level inside its
 // timer, the scan_frt_csc_cuda_mono calls, pre_update_bc_cuda and
-// update_bc_cuda.  The engine does the whole source in one search: the first
-// level call runs it (weighted by the root's folded pendants, exporting the
-// depths), the later calls return the per-level counts it found, and
-// update_bc_cuda has nothing left to do.
+// update_bc_cuda.  Each source costs one slot of a searched-ahead batch: the
+// first level call finds (or searches) it, the later calls return the
+// per-level counts it found, and update_bc_cuda adds its dependencies,
+// weighted by the root's folded pendants, into bc.
 void set_mlp_cuda(LOCINT row, int, int) {
     g_v0 = row;
     g_pending = true;
+    g_committed = false;
     g_count.clear();
 }
 
-static void run_source() {
-    const double mult = (double)g_reach_v0 + 1.0;
-    bcg_stats st{};
-    int rc = bcg_run_root_levels(g_graph, g_v0, mult, g_reach_v0, g_level.data(), &st);
-    if (rc) fail("scan_col_csc_cuda_mono", rc);
+static void search_source() {
+    const uint32_t n = (uint32_t)g_deg.size();
+    uint32_t slot = kAhead;
+    for (uint32_t k = 0; k < g_ahead.nroots; ++k)
+        if (g_ahead.roots[k] == g_v0) slot = k;
+    if (slot == kAhead) {
+        // a new batch: this source and the next candidates of the driver's order
+        uint32_t nr = 0;
+        g_ahead.roots[nr++] = g_v0;
+        for (uint32_t v = g_v0 + 1; v < n && nr < kAhead; ++v)
+            if (g_deg[v]) g_ahead.roots[nr++] = v;
+        g_ahead.nroots = 0;
+        int rc = bcg_run_slots(g_graph, kAhead, g_ahead.roots, nr, g_ahead.d_delta, g_ahead.level.data(),
+                               g_ahead.visited, g_ahead.wsum);
+        if (rc) fail("scan_col_csc_cuda_mono", rc);
+        g_ahead.nroots = nr;
+        slot = 0;
+    }
+    g_slot = slot;
     g_pending = false;
     g_count.clear();
-    for (int32_t l : g_level) {
+    const int32_t *lv = g_ahead.level.data() + (size_t)slot * n;
+    for (uint32_t v = 0; v < n; ++v) {
+        const int32_t l = lv[v];
         if (l < 0) continue;
         if ((size_t)l >= g_count.size()) g_count.resize(l + 1, 0);
         ++g_count[l];
     }
-    // comp_vertices = sum of (1 + reach) over the reached vertices
-    g_reach_visited = st.comp_vertices - st.visited - g_reach_v0;
+    // wsum = sum of (1 + reach) over the reached vertices
+    g_reach_visited = g_ahead.wsum[slot] - g_ahead.visited[slot] - g_reach_v0;
 }
 
 LOCINT scan_col_csc_cuda_mono(int, int level) {
-    if (g_pending) run_source();
+    if (g_pending) search_source();
     return (level >= 0 && (size_t)level < g_count.size()) ? g_count[level] : 0u;
 }
 
 LOCINT scan_frt_csc_cuda_mono(int, int ncol, int) { return (LOCINT)ncol; }
 
 void pre_update_bc_cuda(LOCINT *, uint64_t, LOCINT *all) {
-    if (g_pending) run_source();
+    if (g_pending) search_source();
     *all = (LOCINT)g_reach_visited;
 }
 
+// bc[v] += (reach_v0 + 1) * delta_v0(v) for v != v0 and the source term
+// bc[v0] += reach_v0 * (W - 2) (update_bc, cuda_kernels.cu:263-277, without
+// its contributions to unreached vertices: the definition's bc).
 void update_bc_cuda(uint64_t, int, const uint64_t) {
-    if (g_pending) run_source();  // a driver that skipped the level calls
+    if (g_pending) search_source();  // a driver that skipped the level calls
+    if (g_committed) return;
+    const uint64_t W = g_ahead.wsum[g_slot];
+    const double root_add = (g_reach_v0 && W >= 2) ? (double)g_reach_v0 * (double)(W - 2) : 0.0;
+    const size_t n = g_deg.size();
+    int rc = bcg_add_scaled(g_graph, g_ahead.d_delta + (size_t)g_slot * n, (double)g_reach_v0 + 1.0, g_v0, root_add);
+    if (rc) fail("update_bc_cuda", rc);
+    g_committed = true;
 }
 
 void get_msk(LOCINT *msk) {
-    const size_t n = g_level.size();
+    const size_t n = g_deg.size();
+    const int32_t *lv = g_ahead.level.data() + (size_t)g_slot * n;
     memset(msk, 0, ((n + 31) / 32) * sizeof(uint32_t));
     for (size_t v = 0; v < n; ++v)
-        if (g_level[v] >= 0) msk[v / 32] |= 1u << (v % 32);
+        if (lv[v] >= 0) msk[v / 32] |= 1u << (v % 32);
 }
 
 void get_bc(float *bc) {
@@ -121,6 +170,8 @@ void get_bc(float *bc) {
 void fincuda(void) {
     if (g_graph) bcg_graph_destroy(g_graph);
     g_graph = nullptr;
+    cudaFree(g_ahead.d_delta);
+    g_ahead = Ahead{};
 }
 
 void *CudaMallocHostSet(size_t size, int val) {

@@ -225,6 +225,7 @@ static void graph_free(bcg_graph *g) {
     tree_free(g);
     cudaFree(g->d_vinfo_trees);
     cudaFree(g->d_level_out);
+    cudaFree(g->d_slot_level);
     cudaFree(g->d_ext);
     cudaFree(g->d_rows); cudaFree(g->d_ctrl);
     cudaFree(g->d_roots); cudaFree(g->d_pend); cudaFree(g->d_mult); cudaFree(g->d_rstat);
@@ -400,16 +401,19 @@ struct RunPlan {
     uint64_t skipped = 0;
     // trees mode: sources in components that are trees (no search needed)
     uint64_t tree_only = 0, tree_edges = 0, tree_verts = 0;
+    uint64_t launches = 0;  // kernels the planning launched (the source gather)
 };
 
 // Trees mode: the closed-form bc of the tree vertices (and the anchors' tree
 // terms) for this run's sources, added on the device after the search.
 static int add_tree_terms(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *stats) {
-    const int rc = tree_terms(g, st);
+    uint64_t nl = 0;
+    const int rc = tree_terms(g, st, &nl);
     if (rc) return rc;
     if (stats) {
         stats->teps_edges += p.tree_edges;
         stats->comp_vertices += p.tree_verts;
+        stats->launches += nl;
     }
     return BCG_OK;
 }
@@ -424,6 +428,7 @@ static int plan_run(bcg_graph *g, const uint32_t *src, uint64_t nsrc, RunPlan &p
     if (g->trees) {
         const int rc = tree_source_info(g, src, nsrc, info, st);
         if (rc) return rc;
+        if (nsrc) p.launches += 1;
     }
     std::unordered_map<uint32_t, uint32_t> idx;
     idx.reserve(nsrc * 2 + 1);
@@ -500,12 +505,15 @@ struct DebugOut {
     double *delta = nullptr;
 };
 
-static int run_plan(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *stats, const DebugOut &dbg) {
+// rs_out (with stats): every root's own totals, in plan order.
+static int run_plan(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *stats, const DebugOut &dbg,
+                    std::vector<RootStat> *rs_out = nullptr) {
     const bool debug = dbg.width != 0;
     const uint64_t nroots = p.roots.size();
     if (stats) {
         stats->skipped = p.skipped;
         stats->roots = nroots;
+        stats->launches = p.launches;
     }
     if (nroots == 0) return BCG_OK;
     const uint32_t S = debug ? dbg.width : choose_width(g, nroots);
@@ -569,6 +577,7 @@ static int run_plan(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *
             int grid = 0;
             rc = launch_sweep((int)S, a, st, &grid, ext);
             if (rc) return rc;
+            if (stats) ++stats->launches;
             if (b0 + nb < nbatch) {
                 // errors of this launch are read before the control block is reused
                 CK(cudaStreamSynchronize(st));
@@ -621,6 +630,7 @@ static int run_plan(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *
     if (stats) {
         std::vector<RootStat> rs(slots);
         CK(cudaMemcpy(rs.data(), g->d_rstat, slots * sizeof(RootStat), cudaMemcpyDeviceToHost));
+        if (rs_out) rs_out->assign(rs.begin(), rs.begin() + nroots);
         uint64_t teps = 0, vis = 0, cv = 0, se = 0;
         uint32_t md = 0;
         for (uint64_t i = 0; i < nroots; ++i) {
@@ -1067,6 +1077,64 @@ int bcg_run_weighted(bcg_graph *g, const uint32_t *roots, const double *mult, co
         p.count.push_back(1);
     }
     return run_plan(g, p, 0, st, DebugOut{});
+}
+
+// bc[v] += mult * delta[v] for v != root, bc[root] += root_add.
+__global__ void k_add_scaled(uint32_t n, double *__restrict__ bc, const double *__restrict__ delta, double mult,
+                             uint32_t root, double root_add) {
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    bc[v] += (v == root) ? root_add : mult * delta[v];
+}
+
+int bcg_run_slots(bcg_graph *g, uint32_t width, const uint32_t *roots, uint32_t nroots, double *d_delta,
+                  int32_t *level, uint64_t *visited, uint64_t *wsum) {
+    clear_error();
+    if (!g || (nroots && !roots) || !d_delta) return set_error(BCG_ERR_ARG, "null argument");
+    if (g->trees) return set_error(BCG_ERR_ARG, "graph was created with BCG_PRUNE_TREES");
+    if (width != 1 && width != 3 && width != 6) return set_error(BCG_ERR_ARG, "batch width %u not in {1,3,6}", width);
+    if (nroots == 0 || nroots > width) return set_error(BCG_ERR_ARG, "%u roots for a batch of width %u", nroots, width);
+    const size_t n = g->n, cells = n * width;
+    RunPlan p;
+    for (uint32_t k = 0; k < nroots; ++k) {
+        if (roots[k] >= g->n) return set_error(BCG_ERR_ARG, "root %u >= n=%u", roots[k], g->n);
+        p.roots.push_back(roots[k]);
+        p.pend.push_back(0);
+        p.mult.push_back(0.0);  // nothing is added to bc: the dependencies go to d_delta
+        p.count.push_back(1);
+    }
+    if (g->slot_level_cap < cells) {
+        cudaFree(g->d_slot_level);
+        g->d_slot_level = nullptr;
+        g->slot_level_cap = 0;
+        CK(cudaMalloc(&g->d_slot_level, cells * sizeof(int32_t)));
+        g->slot_level_cap = cells;
+    }
+    CK(cudaMemsetAsync(d_delta, 0, cells * sizeof(double), 0));
+    DebugOut out;
+    out.width = width;
+    out.level = g->d_slot_level;
+    out.delta = d_delta;
+    bcg_stats st{};
+    std::vector<RootStat> rs;
+    int rc = run_plan(g, p, 0, &st, out, &rs);
+    if (rc) return rc;
+    if (level) CK(cudaMemcpy(level, g->d_slot_level, (size_t)nroots * n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    for (uint32_t k = 0; k < nroots; ++k) {
+        if (visited) visited[k] = rs[k].visited;
+        if (wsum) wsum[k] = rs[k].wsum;
+    }
+    return BCG_OK;
+}
+
+int bcg_add_scaled(bcg_graph *g, const double *d_delta, double mult, uint32_t root, double root_add) {
+    clear_error();
+    if (!g || !d_delta) return set_error(BCG_ERR_ARG, "null argument");
+    if (root >= g->n) return set_error(BCG_ERR_ARG, "root %u >= n=%u", root, g->n);
+    const uint32_t n = g->n;
+    k_add_scaled<<<(n + 255) / 256, 256>>>(n, g->d_bc, d_delta, mult, root, root_add);
+    CK(cudaGetLastError());
+    return BCG_OK;
 }
 
 int bcg_run_root_levels(bcg_graph *g, uint32_t root, double mult, uint32_t pend, int32_t *level,

@@ -74,6 +74,8 @@ struct bcg_graph {
     bcg::TreeDev tdev;
     uint2 *d_vinfo_trees = nullptr;   // degree/reach words built by the peeling (until creation ends)
     int32_t *d_level_out = nullptr;   // depths exported by bcg_run_root_levels
+    int32_t *d_slot_level = nullptr;  // depths exported by bcg_run_slots (width * n)
+    size_t slot_level_cap = 0;
     // Trees mode numbers the searched vertices internally: the vertices with
     // kept edges first (caller's order), then the rest, so the tiles cover
     // [0, tile_n) only.  tdev.intl: caller's id -> internal id; d_ext:
@@ -137,8 +139,9 @@ int prepare_trees(bcg_graph *g, const uint32_t *d_offs0, const uint32_t *d_adj0,
 int tree_source_info(bcg_graph *g, const uint32_t *src, uint64_t k, std::vector<uint4> &info, cudaStream_t st);
 // Adds the closed-form betweenness of the tree vertices (and the anchors'
 // tree terms) for the sources of the last tree_source_info call (duplicates
-// count; sources of degree 0 add nothing) into g's bc, on stream st.
-int tree_terms(bcg_graph *g, cudaStream_t st);
+// count; sources of degree 0 add nothing) into g's bc, on stream st;
+// *launches counts its kernels.
+int tree_terms(bcg_graph *g, cudaStream_t st, uint64_t *launches);
 void tree_free(bcg_graph *g);
 // Uploads ngraphs host CSR graphs as one disjoint union (graph order[p] at
 // union position p, its vertex v at base[order[p]] + v; with by_active the

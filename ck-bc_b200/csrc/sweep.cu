@@ -249,10 +249,7 @@ struct WarpSmem {
     alignas(16) uint2 vbuf[2][kTileVerts + 2];   // their {degree, reach} words, from an even vertex on
     alignas(16) uint32_t obuf[2][kTileVerts + 8];  // their row starts, from a multiple-of-4 vertex on
     unsigned long long mbar[2];              // completion of the four copies of buffer b
-    uint32_t pre[kTileVerts + 1];            // exclusive scan of the vertices' segment counts
-    uint32_t eb[kTileVerts];                 // start of vertex j's edges in its adjs buffer
-    uint32_t dg[kTileVerts];                 // vertex j's edges in this sweep (0: none)
-    uint32_t mask[kTileVerts];               // active slots of vertex j
+    uint4 vmeta[kTileVerts];                 // {first segment, edge start in adjs, edges, active slots}
     unsigned long long part[32][S];          // the round's segment partial sums, by lane
     unsigned char sown[kTileEdges / kItems + kTileVerts];  // vertex of each segment of the tile
     uint32_t app[2 * 32];   // buffered appends to the next level's list
@@ -574,13 +571,13 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
         if (ee < eb) ee = eb;
         if (m) dg = ee - eb;
         if (MODE == kBwd && d == x.D) dg = 0;
-        ws.eb[lane] = eb - ab;
-        ws.dg[lane] = dg;
+        ws.vmeta[lane].y = eb - ab;
+        ws.vmeta[lane].z = dg;
         if (MODE == kFwdPush) {
 #pragma unroll
             for (int k = 0; k < S; ++k) ws.own[lane][k] = ((m >> k) & 1u) ? w_val<S>(ow, k) : 0ull;
         }
-        ws.mask[lane] = m;
+        ws.vmeta[lane].w = m;
     }
     if (hub && !__shfl_sync(0xffffffffu, m, 0)) return;  // same decision in every chunk
     // segment prefix
@@ -592,8 +589,7 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
         if (lane >= (unsigned)o) incl += y;
     }
     const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-    if (lane < nv) ws.pre[lane] = incl - nseg;
-    if (lane == 0) ws.pre[nv] = total;
+    if (lane < nv) ws.vmeta[lane].x = incl - nseg;
     // segment -> vertex map (one-vertex tiles need none)
     if (nv > 1)
         for (uint32_t p = incl - nseg; p < incl; ++p) ws.sown[p] = (unsigned char)lane;
@@ -612,17 +608,18 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
 #pragma unroll
     for (int k = 0; k < S; ++k) ls[k] = 0ull;
     // the lane's own vertex: its segments and the running fold of their sums
-    const uint32_t myp0 = (lane < nv) ? ws.pre[lane] : 0u, myp1 = (lane < nv) ? ws.pre[lane + 1] : 0u;
+    const uint32_t myp0 = incl - nseg, myp1 = incl;
     for (uint32_t r0 = s0; r0 < s1; r0 += 32) {
         const uint32_t seg = r0 + lane;
         const bool has = seg < s1;
         uint32_t j = 0, cnt = 0, e0 = 0, jm = 0;
         if (has) {
             j = solo ? 0u : ws.sown[seg];
-            const uint32_t rr = (seg - ws.pre[j]) * kItems;
-            cnt = min((uint32_t)kItems, ws.dg[j] - rr);
-            e0 = ws.eb[j] + rr;
-            jm = ws.mask[j];
+            const uint4 vm = ws.vmeta[j];
+            const uint32_t rr = (seg - vm.x) * kItems;
+            cnt = min((uint32_t)kItems, vm.z - rr);
+            e0 = vm.y + rr;
+            jm = vm.w;
         }
         uint32_t uu[kItems];
 #pragma unroll

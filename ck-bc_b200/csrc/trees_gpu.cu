@@ -218,11 +218,13 @@ __global__ void k_tp_len(uint32_t n, const uint32_t *__restrict__ ext, const uin
 }
 
 // The kept lists in internal ids (one warp per live vertex; order kept, and
-// the numbering is monotone on live vertices, so lists stay sorted).
+// the numbering is monotone on live vertices, so lists stay sorted).  A
+// neighbour u of a live vertex is kept exactly when it is live itself
+// (intl[u] < nlive): a kept neighbour has that kept edge, a peeled one has no
+// kept edge at all.
 __global__ void k_tp_fill(uint32_t nlive, const uint32_t *__restrict__ ext, const uint32_t *__restrict__ offs,
-                          const uint32_t *__restrict__ adj, const uint32_t *__restrict__ rem,
-                          const uint32_t *__restrict__ intl, const uint32_t *__restrict__ offs2,
-                          uint32_t *__restrict__ adj2) {
+                          const uint32_t *__restrict__ adj, const uint32_t *__restrict__ intl,
+                          const uint32_t *__restrict__ offs2, uint32_t *__restrict__ adj2) {
     const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const unsigned lane = threadIdx.x & 31;
     if (w >= nlive) return;
@@ -230,14 +232,11 @@ __global__ void k_tp_fill(uint32_t nlive, const uint32_t *__restrict__ ext, cons
     uint32_t out = offs2[w];
     for (uint32_t b = offs[v]; b < offs[v + 1]; b += 32) {
         const uint32_t e = b + lane;
-        uint32_t u = 0;
-        bool keep = false;
-        if (e < offs[v + 1]) {
-            u = adj[e];
-            keep = rem[u] == kKept;
-        }
+        uint32_t iu = nlive;
+        if (e < offs[v + 1]) iu = intl[adj[e]];
+        const bool keep = iu < nlive;
         const unsigned bal = __ballot_sync(0xffffffffu, keep);
-        if (keep) adj2[out + __popc(bal & ((1u << lane) - 1u))] = intl[u];
+        if (keep) adj2[out + __popc(bal & ((1u << lane) - 1u))] = iu;
         out += __popc(bal);
     }
 }
@@ -336,14 +335,18 @@ __global__ void k_uf_flatten(uint32_t n, uint32_t *root) {
 
 // Component of every vertex (its anchor's root, an internal id) and the
 // vertex count of every component.
+// (Most vertices share a component: the lanes of a warp that do add once.)
 __global__ void k_tp_comp(uint32_t n, const uint32_t *__restrict__ anchor, const uint32_t *__restrict__ intl,
                           const uint32_t *__restrict__ root, uint32_t *__restrict__ comp,
                           unsigned long long *__restrict__ comp_n) {
     const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= n) return;
-    const uint32_t c = root[intl[anchor[v]]];
-    comp[v] = c;
-    atomicAdd(comp_n + c, 1ull);
+    const bool ok = v < n;
+    const uint32_t c = ok ? root[intl[anchor[v]]] : 0u;
+    if (ok) comp[v] = c;
+    const unsigned active = __ballot_sync(0xffffffffu, ok);
+    if (!ok) return;
+    const unsigned peers = __match_any_sync(active, c);
+    if ((threadIdx.x & 31) == (unsigned)(__ffs(peers) - 1)) atomicAdd(comp_n + c, (unsigned long long)__popc(peers));
 }
 
 __global__ void k_check_ids(uint64_t nnz, uint32_t n, const uint32_t *__restrict__ adj, unsigned long long *bad) {
@@ -501,7 +504,7 @@ int prepare_trees(bcg_graph *g, const uint32_t *d_offs0, const uint32_t *d_adj0,
     CKT(cudaMalloc(&g->d_adj, (nnz2 + 4) * sizeof(uint32_t)));
     CKT(cudaMemset(g->d_adj + nnz2, 0, 4 * sizeof(uint32_t)));
     if (nlive)
-        k_tp_fill<<<nblocks((uint64_t)nlive * 32, 256), 256, 0, st>>>(nlive, g->d_ext, d_offs0, d_adj0, rem, intl,
+        k_tp_fill<<<nblocks((uint64_t)nlive * 32, 256), 256, 0, st>>>(nlive, g->d_ext, d_offs0, d_adj0, intl,
                                                                       g->d_offs, g->d_adj);
     CKT(cudaGetLastError());
     // degree/reach words (internal ids), kept for create_common's buffer
@@ -573,25 +576,33 @@ int tree_source_info(bcg_graph *g, const uint32_t *src, uint64_t k, std::vector<
     return BCG_OK;
 }
 
-int tree_terms(bcg_graph *g, cudaStream_t st) {
+int tree_terms(bcg_graph *g, cudaStream_t st, uint64_t *launches) {
     TreeDev &t = g->tdev;
     const uint32_t n = g->n;
     const uint64_t k = t.nsrc;
+    *launches = 0;
     if (k == 0) return BCG_OK;
     CKT(cudaMemsetAsync(t.cnt, 0, (size_t)n * sizeof(uint32_t), st));
     CKT(cudaMemsetAsync(t.csrc, 0, (size_t)n * sizeof(unsigned long long), st));
     CKT(cudaMemsetAsync(t.acc, 0, (size_t)n * sizeof(unsigned long long), st));
     k_tt_count<<<nblocks(k, 256), 256, 0, st>>>(k, t.src, t.cnt);
     k_tt_init<<<nblocks(n, 256), 256, 0, st>>>(n, t.cnt, t.comp, t.sub, t.csrc);
+    uint64_t nl = 3;  // count, init, add
     for (size_t r = 0; r + 1 < t.round_off.size(); ++r) {
         const uint32_t o = t.round_off[r], c = t.round_off[r + 1] - o;
-        if (c) k_tt_sub<<<nblocks(c, 256), 256, 0, st>>>(c, t.order + o, t.parent, t.sub);
+        if (c) {
+            k_tt_sub<<<nblocks(c, 256), 256, 0, st>>>(c, t.order + o, t.parent, t.sub);
+            ++nl;
+        }
     }
-    if (t.npeeled)
+    if (t.npeeled) {
         k_tt_acc<<<nblocks(t.npeeled, 256), 256, 0, st>>>(t.npeeled, t.order, t.parent, t.sz, t.comp, t.comp_n, t.sub,
                                                           t.csrc, t.acc);
+        ++nl;
+    }
     k_tt_add<<<nblocks(n, 256), 256, 0, st>>>(n, t.acc, g->d_bc);
     CKT(cudaGetLastError());
+    *launches = nl;
     return BCG_OK;
 }
 

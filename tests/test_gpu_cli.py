@@ -98,16 +98,19 @@ def test_cli_generated_rmat(tmp_path):
 
 @pytest.mark.skipif(not os.path.exists(REF_ON_BCG), reason="reference host driver not linked (needs the "
                                                             "reference sources at build time)")
-def test_reference_host_driver_over_compat(graph_file, tmp_path):
-    """The reference's unmodified bc2d.c linked against libbc2d_compat.so."""
+@pytest.mark.parametrize("start,count", [(0, 200), (37, 53)])
+def test_reference_host_driver_over_compat(graph_file, tmp_path, start, count):
+    """The reference's unmodified bc2d.c linked against libbc2d_compat.so.  The
+    shim searches sources six at a time ahead of the driver; a range that
+    ends inside such a batch must leave the candidates past its end out."""
     path, offs, adj = graph_file
     n = len(offs) - 1
     out = str(tmp_path / "refres")
-    r = subprocess.run([REF_ON_BCG, "-p", "1x1", "-f", path, "-n", str(n), "-N", "200", "-o", out],
-                       capture_output=True, text=True, timeout=600, cwd=str(tmp_path))
+    r = subprocess.run([REF_ON_BCG, "-p", "1x1", "-f", path, "-n", str(n), "-r", str(start), "-N", str(count),
+                        "-o", out], capture_output=True, text=True, timeout=600, cwd=str(tmp_path))
     assert r.returncode == 0, r.stderr[-2000:]
     _, ids, vals = _read_result(out + "_1X1_0.log")
-    ref, _ = oracle.bc(offs, adj, np.arange(200, dtype=np.uint32))
+    ref, _ = oracle.bc(offs, adj, np.arange(start, start + count, dtype=np.uint32))
     # float32 get_bc and "%.2f" output (cuda_kernels.cu:1039-1041, bc2d.c:1065)
     assert np.all(np.abs(vals - ref / 2) <= 0.005 + 2e-7 * np.abs(ref))
 
