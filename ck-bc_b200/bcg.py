@@ -110,8 +110,8 @@ SIGNATURES = {
                                            _i32p, ctypes.POINTER(Stats)]),
     "bcg_run_slots": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, _u32p, ctypes.c_uint32, ctypes.c_void_p,
                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
-    "bcg_add_scaled": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_uint32,
-                                      ctypes.c_double]),
+    "bcg_add_scaled": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, _u32p,
+                                      ctypes.POINTER(ctypes.c_double), _u32p, ctypes.POINTER(ctypes.c_double)]),
     "bcg_set_batch_width": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32]),
     "bcg_set_sigma_mode": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "bcg_single_source_ext": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, _i32p, _u64p, _f64p]),

@@ -3,6 +3,7 @@
 // MY_CUDA_CHECK (cudamacro.h:1-7), since the ABI has no status returns.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cinttypes>
 #include <cstdio>
 #include <cstdlib>
@@ -29,23 +30,40 @@ uint64_t g_reach_visited = 0;      // sum of reach over the vertices it reached,
 
 // Sources searched ahead: the driver asks for its sources one at a time, in
 // increasing order, skipping degree 0 (bc2d.c:1016-1036), so the first
-// source of a batch is searched together with the next kAhead - 1 candidates
-// (bcg_run_slots: nothing added to bc).  A source's dependencies are added
-// when the driver commits it (update_bc_cuda); a candidate it never asks
-// for is dropped.
-constexpr uint32_t kAhead = 6;
+// source of a block is searched together with the next candidates of that
+// order, in batches of 6 in one launch (bcg_run_slots: nothing added to
+// bc).  The driver commits each source in update_bc_cuda; the commits are
+// added to bc in that order by one kernel when the next block is searched
+// or bc is read (bcg_add_scaled).  A candidate it never asks for is dropped.
+constexpr uint32_t kWidth = 6;
+constexpr uint32_t kMaxAhead = 30;               // five batches
+constexpr size_t kAheadBytes = 64ull << 20;      // depths + dependencies of a block
 struct Ahead {
+    uint32_t cap = kWidth;                       // roots per block (a multiple of kWidth)
     uint32_t nroots = 0;
-    uint32_t roots[kAhead] = {};
-    uint64_t visited[kAhead] = {}, wsum[kAhead] = {};
-    std::vector<int32_t> level;  // kAhead * n depths (-1 = not reached)
-    double *d_delta = nullptr;   // kAhead * n dependencies on the device
+    uint32_t roots[kMaxAhead] = {};
+    uint64_t visited[kMaxAhead] = {}, wsum[kMaxAhead] = {};
+    std::vector<int32_t> level;                  // cap * n depths (-1 = not reached)
+    double *d_delta = nullptr;                   // cap * n dependencies on the device
+    // committed sources not yet added to bc
+    uint32_t ncommit = 0;
+    uint32_t cslot[kMaxAhead] = {}, croot[kMaxAhead] = {};
+    double cmult[kMaxAhead] = {}, cadd[kMaxAhead] = {};
 } g_ahead;
 uint32_t g_slot = 0;               // the current source's slot in g_ahead
+
 
 [[noreturn]] void fail(const char *what, int rc) {
     fprintf(stderr, "bc2d_compat: %s failed (%d): %s\n", what, rc, bcg_last_error());
     exit(EXIT_FAILURE);
+}
+
+void flush_commits() {
+    if (!g_ahead.ncommit) return;
+    int rc = bcg_add_scaled(g_graph, g_ahead.d_delta, g_ahead.ncommit, g_ahead.cslot, g_ahead.cmult, g_ahead.croot,
+                            g_ahead.cadd);
+    if (rc) fail("update_bc_cuda", rc);
+    g_ahead.ncommit = 0;
 }
 
 }  // namespace
@@ -59,9 +77,13 @@ size_t initcuda(uint64_t ned, LOCINT *col, LOCINT *row) {
     g_deg.resize(n);
     for (uint32_t v = 0; v < n; ++v) g_deg[v] = col[v + 1] - col[v];
     g_ahead = Ahead{};
-    g_ahead.level.assign((size_t)kAhead * n, -1);
-    if (cudaMalloc(&g_ahead.d_delta, (size_t)kAhead * n * sizeof(double)) != cudaSuccess) {
-        fprintf(stderr, "bc2d_compat: initcuda: cudaMalloc of %zu bytes failed\n", (size_t)kAhead * n * sizeof(double));
+    const size_t per_root = (size_t)n * (sizeof(double) + sizeof(int32_t));
+    size_t cap = kAheadBytes / per_root / kWidth * kWidth;
+    g_ahead.cap = (uint32_t)std::min<size_t>(kMaxAhead, std::max<size_t>(kWidth, cap));
+    g_ahead.level.assign((size_t)g_ahead.cap * n, -1);
+    if (cudaMalloc(&g_ahead.d_delta, (size_t)g_ahead.cap * n * sizeof(double)) != cudaSuccess) {
+        fprintf(stderr, "bc2d_compat: initcuda: cudaMalloc of %zu bytes failed\n",
+                (size_t)g_ahead.cap * n * sizeof(double));
         exit(EXIT_FAILURE);
     }
     printf("ROWBL = %i - ROWPP = %i\n", (int)n, (int)n);
@@ -83,10 +105,11 @@ void setcuda(uint64_t, LOCINT *, LOCINT *, LOCINT reach_v0) {
 // The driver's per-source sequence (bc_func_mono, bc2d.c:504-580) is
 // setcuda, set_mlp_cuda, then scan_col_csc_cuda_mono per level inside its
 // timer, the scan_frt_csc_cuda_mono calls, pre_update_bc_cuda and
-// update_bc_cuda.  Each source costs one slot of a searched-ahead batch: the
+// update_bc_cuda.  Each source costs one slot of a searched-ahead block: the
 // first level call finds (or searches) it, the later calls return the
-// per-level counts it found, and update_bc_cuda adds its dependencies,
-// weighted by the root's folded pendants, into bc.
+// per-level counts it found, and update_bc_cuda commits its dependencies,
+// weighted by the root's folded pendants (added to bc with the block's other
+// commits, in commit order).
 void set_mlp_cuda(LOCINT row, int, int) {
     g_v0 = row;
     g_pending = true;
@@ -96,17 +119,19 @@ void set_mlp_cuda(LOCINT row, int, int) {
 
 static void search_source() {
     const uint32_t n = (uint32_t)g_deg.size();
-    uint32_t slot = kAhead;
+    uint32_t slot = kMaxAhead;
     for (uint32_t k = 0; k < g_ahead.nroots; ++k)
         if (g_ahead.roots[k] == g_v0) slot = k;
-    if (slot == kAhead) {
-        // a new batch: this source and the next candidates of the driver's order
+    if (slot == kMaxAhead) {
+        // a new block: this source and the next candidates of the driver's
+        // order (the block's dependencies are about to be overwritten)
+        flush_commits();
         uint32_t nr = 0;
         g_ahead.roots[nr++] = g_v0;
-        for (uint32_t v = g_v0 + 1; v < n && nr < kAhead; ++v)
+        for (uint32_t v = g_v0 + 1; v < n && nr < g_ahead.cap; ++v)
             if (g_deg[v]) g_ahead.roots[nr++] = v;
         g_ahead.nroots = 0;
-        int rc = bcg_run_slots(g_graph, kAhead, g_ahead.roots, nr, g_ahead.d_delta, g_ahead.level.data(),
+        int rc = bcg_run_slots(g_graph, kWidth, g_ahead.roots, nr, g_ahead.d_delta, g_ahead.level.data(),
                                g_ahead.visited, g_ahead.wsum);
         if (rc) fail("scan_col_csc_cuda_mono", rc);
         g_ahead.nroots = nr;
@@ -138,17 +163,19 @@ void pre_update_bc_cuda(LOCINT *, uint64_t, LOCINT *all) {
     *all = (LOCINT)g_reach_visited;
 }
 
-// bc[v] += (reach_v0 + 1) * delta_v0(v) for v != v0 and the source term
-// bc[v0] += reach_v0 * (W - 2) (update_bc, cuda_kernels.cu:263-277, without
-// its contributions to unreached vertices: the definition's bc).
+// Commits bc[v] += (reach_v0 + 1) * delta_v0(v) for v != v0 and the source
+// term bc[v0] += reach_v0 * (W - 2) (update_bc, cuda_kernels.cu:263-277,
+// without its contributions to unreached vertices: the definition's bc).
 void update_bc_cuda(uint64_t, int, const uint64_t) {
     if (g_pending) search_source();  // a driver that skipped the level calls
     if (g_committed) return;
+    if (g_ahead.ncommit == kMaxAhead) flush_commits();  // a driver that repeats sources
     const uint64_t W = g_ahead.wsum[g_slot];
-    const double root_add = (g_reach_v0 && W >= 2) ? (double)g_reach_v0 * (double)(W - 2) : 0.0;
-    const size_t n = g_deg.size();
-    int rc = bcg_add_scaled(g_graph, g_ahead.d_delta + (size_t)g_slot * n, (double)g_reach_v0 + 1.0, g_v0, root_add);
-    if (rc) fail("update_bc_cuda", rc);
+    const uint32_t j = g_ahead.ncommit++;
+    g_ahead.cslot[j] = g_slot;
+    g_ahead.croot[j] = g_v0;
+    g_ahead.cmult[j] = (double)g_reach_v0 + 1.0;
+    g_ahead.cadd[j] = (g_reach_v0 && W >= 2) ? (double)g_reach_v0 * (double)(W - 2) : 0.0;
     g_committed = true;
 }
 
@@ -161,6 +188,7 @@ void get_msk(LOCINT *msk) {
 }
 
 void get_bc(float *bc) {
+    flush_commits();
     std::vector<double> b(g_deg.size());
     int rc = bcg_get_bc(g_graph, b.data());
     if (rc) fail("get_bc", rc);

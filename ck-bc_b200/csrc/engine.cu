@@ -217,18 +217,19 @@ static void graph_free(bcg_graph *g) {
     int cur = -1;
     cudaGetDevice(&cur);
     if (cur != g->device) cudaSetDevice(g->device);
-    cudaFree(g->d_offs); cudaFree(g->d_adj); cudaFree(g->d_vinfo);
-    cudaFree(g->d_anchor); cudaFree(g->d_reach); cudaFree(g->d_bc);
-    cudaFree(g->d_tiles); cudaFree(g->d_hub_acc); cudaFree(g->d_hub_cnt);
-    cudaFree(g->d_tile_of); cudaFree(g->d_tmark); cudaFree(g->d_lists);
-    cudaFree(g->d_lbase); cudaFree(g->d_lcnt); cudaFree(g->d_ulist); cudaFree(g->d_bc_save);
+    cudaDeviceSynchronize();  // work on any stream may still read the buffers
+    dev_free(g->d_offs); dev_free(g->d_adj); dev_free(g->d_vinfo);
+    dev_free(g->d_anchor); dev_free(g->d_reach); dev_free(g->d_bc);
+    dev_free(g->d_tiles); dev_free(g->d_hub_acc); dev_free(g->d_hub_cnt);
+    dev_free(g->d_tile_of); dev_free(g->d_tmark); dev_free(g->d_lists);
+    dev_free(g->d_lbase); dev_free(g->d_lcnt); dev_free(g->d_ulist); dev_free(g->d_bc_save);
     tree_free(g);
-    cudaFree(g->d_vinfo_trees);
-    cudaFree(g->d_level_out);
-    cudaFree(g->d_slot_level);
-    cudaFree(g->d_ext);
-    cudaFree(g->d_rows); cudaFree(g->d_ctrl);
-    cudaFree(g->d_roots); cudaFree(g->d_pend); cudaFree(g->d_mult); cudaFree(g->d_rstat);
+    dev_free(g->d_vinfo_trees);
+    dev_free(g->d_level_out);
+    dev_free(g->d_slot_level);
+    dev_free(g->d_ext);
+    dev_free(g->d_rows); dev_free(g->d_ctrl);
+    dev_free(g->d_roots); dev_free(g->d_pend); dev_free(g->d_mult); dev_free(g->d_rstat);
     if (g->ev0) cudaEventDestroy(g->ev0);
     if (g->ev1) cudaEventDestroy(g->ev1);
     if (cur >= 0 && cur != g->device) cudaSetDevice(cur);
@@ -237,32 +238,36 @@ static void graph_free(bcg_graph *g) {
 
 int ensure_state(bcg_graph *g, uint32_t S) {
     if (g->state_width >= S) return BCG_OK;  // row_bytes grows with S
-    cudaFree(g->d_rows); g->d_rows = nullptr;
-    cudaFree(g->d_hub_acc); g->d_hub_acc = nullptr;
-    cudaFree(g->d_lists); g->d_lists = nullptr;
+    CK(cudaDeviceSynchronize());  // earlier runs (any stream) are done with the old buffers
+    dev_free(g->d_rows); g->d_rows = nullptr;
+    dev_free(g->d_hub_acc); g->d_hub_acc = nullptr;
+    dev_free(g->d_lists); g->d_lists = nullptr;
     g->state_width = 0;
-    CK(cudaMalloc(&g->d_rows, (size_t)g->n * row_bytes((int)S)));
+    CK(dev_alloc(&g->d_rows, (size_t)g->n * row_bytes((int)S)));
     // one slot per hub chunk, written by the chunk before it is read
-    CK(cudaMalloc(&g->d_hub_acc, (size_t)std::max(1u, g->nhubchunks) * S * sizeof(unsigned long long)));
+    CK(dev_alloc(&g->d_hub_acc, (size_t)std::max(1u, g->nhubchunks) * S * sizeof(unsigned long long)));
     // every (tile, level) pair is listed at most once per batch: a tile is on
     // level d's list only if one of its vertices (or chunks) first reaches d,
     // so the lists of one batch hold at most S * (n + ntiles) entries
     g->list_cap = (unsigned long long)S * ((unsigned long long)g->n + g->ntiles);
-    CK(cudaMalloc(&g->d_lists, g->list_cap * sizeof(uint32_t)));
+    CK(dev_alloc(&g->d_lists, g->list_cap * sizeof(uint32_t)));
+    CK(cudaDeviceSynchronize());  // the new buffers are ready for any stream
     g->state_width = S;
     return BCG_OK;
 }
 
 static int ensure_run(bcg_graph *g, size_t slots) {
     if (g->run_cap >= slots) return BCG_OK;
-    cudaFree(g->d_roots); cudaFree(g->d_pend); cudaFree(g->d_mult); cudaFree(g->d_rstat);
+    CK(cudaDeviceSynchronize());
+    dev_free(g->d_roots); dev_free(g->d_pend); dev_free(g->d_mult); dev_free(g->d_rstat);
     g->d_roots = g->d_pend = nullptr; g->d_mult = nullptr; g->d_rstat = nullptr;
     g->run_cap = 0;
     size_t cap = std::max<size_t>(slots, 64);
-    CK(cudaMalloc(&g->d_roots, cap * sizeof(uint32_t)));
-    CK(cudaMalloc(&g->d_pend, cap * sizeof(uint32_t)));
-    CK(cudaMalloc(&g->d_mult, cap * sizeof(double)));
-    CK(cudaMalloc(&g->d_rstat, cap * sizeof(RootStat)));
+    CK(dev_alloc(&g->d_roots, cap * sizeof(uint32_t)));
+    CK(dev_alloc(&g->d_pend, cap * sizeof(uint32_t)));
+    CK(dev_alloc(&g->d_mult, cap * sizeof(double)));
+    CK(dev_alloc(&g->d_rstat, cap * sizeof(RootStat)));
+    CK(cudaDeviceSynchronize());
     g->run_cap = cap;
     return BCG_OK;
 }
@@ -294,15 +299,16 @@ static int setup_tiles(bcg_graph *g, const uint32_t *h_offs) {
     build_tiles(h_offs, n, g->tile_n ? g->tile_n : n, g->tile_vcap, g->tile_ecap, g->tile_breaks, tiles, g->nhub,
                 g->nhubchunks, tile_of);
     g->ntiles = (uint32_t)tiles.size();
-    CK(cudaMalloc(&g->d_tiles, std::max<size_t>(1, tiles.size()) * sizeof(Tile)));
+    CK(dev_alloc(&g->d_tiles, std::max<size_t>(1, tiles.size()) * sizeof(Tile)));
     if (!tiles.empty())
         CK(cudaMemcpy(g->d_tiles, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice));
-    CK(cudaMalloc(&g->d_tile_of, (size_t)n * sizeof(uint32_t)));
+    CK(dev_alloc(&g->d_tile_of, (size_t)n * sizeof(uint32_t)));
     CK(cudaMemcpy(g->d_tile_of, tile_of.data(), (size_t)n * sizeof(uint32_t), cudaMemcpyHostToDevice));
-    CK(cudaMalloc(&g->d_tmark, std::max<size_t>(1, tiles.size()) * sizeof(uint32_t)));
-    CK(cudaMalloc(&g->d_ulist, 2 * std::max<size_t>(1, tiles.size()) * sizeof(uint32_t)));
-    CK(cudaMalloc(&g->d_hub_cnt, (size_t)std::max(1u, g->nhub) * sizeof(unsigned int)));
+    CK(dev_alloc(&g->d_tmark, std::max<size_t>(1, tiles.size()) * sizeof(uint32_t)));
+    CK(dev_alloc(&g->d_ulist, 2 * std::max<size_t>(1, tiles.size()) * sizeof(uint32_t)));
+    CK(dev_alloc(&g->d_hub_cnt, (size_t)std::max(1u, g->nhub) * sizeof(unsigned int)));
     CK(cudaMemset(g->d_hub_cnt, 0, (size_t)std::max(1u, g->nhub) * sizeof(unsigned int)));
+    CK(cudaDeviceSynchronize());  // the new buffers are ready for any stream
     return BCG_OK;
 }
 
@@ -311,11 +317,11 @@ static int setup_tiles(bcg_graph *g, const uint32_t *h_offs) {
 static int create_common(bcg_graph *g, const uint32_t *h_offs, const uint32_t *h_offs_in) {
     const uint32_t n = g->n;
     // 4 entries of tail padding (the sweep copies 16-byte aligned ranges)
-    CK(cudaMalloc(&g->d_vinfo, ((size_t)n + 4) * sizeof(uint2)));
+    CK(dev_alloc(&g->d_vinfo, ((size_t)n + 4) * sizeof(uint2)));
     CK(cudaMemset(g->d_vinfo, 0, ((size_t)n + 4) * sizeof(uint2)));
-    CK(cudaMalloc(&g->d_bc, (size_t)n * sizeof(double)));
+    CK(dev_alloc(&g->d_bc, (size_t)n * sizeof(double)));
     CK(cudaMemset(g->d_bc, 0, (size_t)n * sizeof(double)));
-    CK(cudaMalloc(&g->d_ctrl, sizeof(Ctrl)));
+    CK(dev_alloc(&g->d_ctrl, sizeof(Ctrl)));
     CK(cudaEventCreate(&g->ev0));
     CK(cudaEventCreate(&g->ev1));
     g->h_deg.resize(n);
@@ -325,8 +331,8 @@ static int create_common(bcg_graph *g, const uint32_t *h_offs, const uint32_t *h
     const bool prune = (g->flags & BCG_PRUNE_DEGREE1) && !(g->flags & BCG_DIRECTED);
     const unsigned nb = (n + 255) / 256;
     if (prune) {
-        CK(cudaMalloc(&g->d_anchor, (size_t)n * sizeof(uint32_t)));
-        CK(cudaMalloc(&g->d_reach, (size_t)n * sizeof(uint32_t)));
+        CK(dev_alloc(&g->d_anchor, (size_t)n * sizeof(uint32_t)));
+        CK(dev_alloc(&g->d_reach, (size_t)n * sizeof(uint32_t)));
         CK(cudaMemset(g->d_reach, 0, (size_t)n * sizeof(uint32_t)));
         k_prune_mark<<<nb, 256>>>(n, g->d_offs, g->d_adj, g->d_anchor, g->d_reach);
         CK(cudaGetLastError());
@@ -345,8 +351,8 @@ static int create_common(bcg_graph *g, const uint32_t *h_offs, const uint32_t *h
         CK(cudaGetLastError());
         g->nnz_pruned = g->nnz;
     }
-    CK(cudaMalloc(&g->d_lbase, (size_t)(kMaxLevel + 3) * sizeof(uint32_t)));
-    CK(cudaMalloc(&g->d_lcnt, (size_t)(kMaxLevel + 3) * sizeof(uint32_t)));
+    CK(dev_alloc(&g->d_lbase, (size_t)(kMaxLevel + 3) * sizeof(uint32_t)));
+    CK(dev_alloc(&g->d_lcnt, (size_t)(kMaxLevel + 3) * sizeof(uint32_t)));
     const int rc = setup_tiles(g, h_offs);
     if (rc) return rc;
     CK(cudaDeviceSynchronize());
@@ -360,8 +366,9 @@ int graph_retile(bcg_graph *g, uint32_t vcap, uint32_t ecap, bool force) {
     if (!force && vcap == g->tile_vcap && ecap == g->tile_ecap) return BCG_OK;
     std::vector<uint32_t> h_offs((size_t)g->n + 1);
     CK(cudaMemcpy(h_offs.data(), g->d_offs, h_offs.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-    cudaFree(g->d_tiles); cudaFree(g->d_tile_of); cudaFree(g->d_tmark); cudaFree(g->d_ulist);
-    cudaFree(g->d_hub_cnt); cudaFree(g->d_hub_acc); cudaFree(g->d_lists);
+    CK(cudaDeviceSynchronize());
+    dev_free(g->d_tiles); dev_free(g->d_tile_of); dev_free(g->d_tmark); dev_free(g->d_ulist);
+    dev_free(g->d_hub_cnt); dev_free(g->d_hub_acc); dev_free(g->d_lists);
     g->d_tiles = nullptr; g->d_tile_of = g->d_tmark = g->d_ulist = g->d_lists = nullptr;
     g->d_hub_cnt = nullptr; g->d_hub_acc = nullptr;
     g->state_width = 0;  // hub accumulators and lists are sized by the tiles
@@ -497,7 +504,8 @@ static void fill_args(bcg_graph *g, BatchArgs &a) {
     a.directed = (g->flags & BCG_DIRECTED) ? 1 : 0;
 }
 
-// Debug outputs of a single-batch run (internal numbering, slot-major).
+// Debug outputs of a run (internal numbering; slot k of batch b at
+// (b * width + k) * n): width = the run's batch width.
 struct DebugOut {
     uint32_t width = 0;  // 0: not a debug run
     int32_t *level = nullptr;
@@ -541,8 +549,8 @@ static int run_plan(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *
     unsigned int *d_tcnt = nullptr;
     const unsigned int trace_cap = 1u << 20;
     if (trace_path && *trace_path) {
-        CK(cudaMalloc(&d_trace, trace_cap * sizeof(TraceRec)));
-        CK(cudaMalloc(&d_tcnt, sizeof(unsigned int)));
+        CK(dev_alloc(&d_trace, trace_cap * sizeof(TraceRec)));
+        CK(dev_alloc(&d_tcnt, sizeof(unsigned int)));
         CK(cudaMemsetAsync(d_tcnt, 0, sizeof(unsigned int), st));
         a.trace = d_trace;
         a.trace_cap = trace_cap;
@@ -554,7 +562,7 @@ static int run_plan(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *
     const bool autoext = g->sigma_mode == 0;
     bool ext = g->sigma_mode == 2;
     if (autoext) {
-        if (!g->d_bc_save) CK(cudaMalloc(&g->d_bc_save, (size_t)g->n * sizeof(double)));
+        if (!g->d_bc_save) CK(dev_alloc(&g->d_bc_save, (size_t)g->n * sizeof(double)));
         CK(cudaMemcpyAsync(g->d_bc_save, g->d_bc, (size_t)g->n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     }
     for (;;) {
@@ -573,6 +581,11 @@ static int run_plan(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *
             a.mult = g->d_mult + b0 * S;
             a.pend = g->d_pend + b0 * S;
             a.rstat = g->d_rstat + b0 * S;
+            // debug outputs: slot k of batch b at ((b * S) + k) * n
+            const size_t dofs = (size_t)b0 * S * a.n;
+            a.dbg_level = dbg.level ? dbg.level + dofs : nullptr;
+            a.dbg_sigma = dbg.sigma ? dbg.sigma + dofs : nullptr;
+            a.dbg_delta = dbg.delta ? dbg.delta + dofs : nullptr;
             a.nbatch = (uint32_t)nb;
             int grid = 0;
             rc = launch_sweep((int)S, a, st, &grid, ext);
@@ -606,8 +619,8 @@ static int run_plan(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *
         Ctrl c{};
         CK(cudaMemcpy(&c, g->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
         if (c.error && c.error != BCG_ERR_OVERFLOW) {
-            cudaFree(d_trace);
-            cudaFree(d_tcnt);
+            dev_free(d_trace);
+            dev_free(d_tcnt);
             return set_error(c.error, "device reported error %d (%s)", c.error,
                              c.error == BCG_ERR_TIMEOUT ? "a bounded wait gave up" : "level limit exceeded");
         }
@@ -618,14 +631,14 @@ static int run_plan(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *
                 ext = true;
                 continue;
             }
-            cudaFree(d_trace);
-            cudaFree(d_tcnt);
+            dev_free(d_trace);
+            dev_free(d_tcnt);
             return set_error(BCG_ERR_OVERFLOW, "a shortest-path count exceeded 2^64");
         }
         break;
     }
-    cudaFree(d_trace);
-    cudaFree(d_tcnt);
+    dev_free(d_trace);
+    dev_free(d_tcnt);
     if (!stats) return BCG_OK;
     if (stats) {
         std::vector<RootStat> rs(slots);
@@ -779,8 +792,8 @@ static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint3
         // 4 entries of tail padding on offsets and adjacency: the sweep copies
         // their ranges in 16-byte aligned pieces that may end up to 12 bytes
         // past the last entry
-        if ((e = cudaMalloc(&g->d_offs, ((size_t)n + 1 + 4) * sizeof(uint32_t))) != cudaSuccess ||
-            (e = cudaMalloc(&g->d_adj, (nnz + 4) * sizeof(uint32_t))) != cudaSuccess)
+        if ((e = dev_alloc(&g->d_offs, ((size_t)n + 1 + 4) * sizeof(uint32_t))) != cudaSuccess ||
+            (e = dev_alloc(&g->d_adj, (nnz + 4) * sizeof(uint32_t))) != cudaSuccess)
             return fail(set_error(BCG_ERR_OOM, "cudaMalloc CSR: %s", cudaGetErrorString(e)));
         const cudaMemcpyKind kind = device_in ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
         if ((e = cudaMemcpy(g->d_offs, offsets, ((size_t)n + 1) * sizeof(uint32_t), kind)) != cudaSuccess ||
@@ -798,7 +811,7 @@ static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint3
         if ((e = cudaMemcpy(g->d_vinfo, g->d_vinfo_trees, (size_t)n * sizeof(uint2), cudaMemcpyDeviceToDevice)) !=
             cudaSuccess)
             return fail(set_error(BCG_ERR_CUDA, "tree weights: %s", cudaGetErrorString(e)));
-        cudaFree(g->d_vinfo_trees);
+        dev_free(g->d_vinfo_trees);
         g->d_vinfo_trees = nullptr;
     }
     *out = g;
@@ -928,11 +941,11 @@ static int debug_batch_impl(bcg_graph *g, uint32_t width, const uint32_t *roots,
     unsigned long long *d_sig = nullptr;
     double *d_del = nullptr;
     int32_t *d_lvl = nullptr;
-    auto cleanup = [&]() { cudaFree(d_save); cudaFree(d_sig); cudaFree(d_del); cudaFree(d_lvl); };
-    if (cudaMalloc(&d_save, n * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&d_sig, cells * sizeof(unsigned long long)) != cudaSuccess ||
-        cudaMalloc(&d_del, cells * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&d_lvl, cells * sizeof(int32_t)) != cudaSuccess) {
+    auto cleanup = [&]() { dev_free(d_save); dev_free(d_sig); dev_free(d_del); dev_free(d_lvl); };
+    if (dev_alloc(&d_save, n * sizeof(double)) != cudaSuccess ||
+        dev_alloc(&d_sig, cells * sizeof(unsigned long long)) != cudaSuccess ||
+        dev_alloc(&d_del, cells * sizeof(double)) != cudaSuccess ||
+        dev_alloc(&d_lvl, cells * sizeof(int32_t)) != cudaSuccess) {
         cleanup();
         return set_error(BCG_ERR_OOM, "debug-batch scratch allocation failed");
     }
@@ -1079,12 +1092,23 @@ int bcg_run_weighted(bcg_graph *g, const uint32_t *roots, const double *mult, co
     return run_plan(g, p, 0, st, DebugOut{});
 }
 
-// bc[v] += mult * delta[v] for v != root, bc[root] += root_add.
-__global__ void k_add_scaled(uint32_t n, double *__restrict__ bc, const double *__restrict__ delta, double mult,
-                             uint32_t root, double root_add) {
+// Roots committed by one bcg_add_scaled call (passed by value).
+constexpr uint32_t kMaxAdd = 64;
+struct AddList {
+    uint32_t count;
+    uint32_t slot[kMaxAdd], root[kMaxAdd];
+    double mult[kMaxAdd], root_add[kMaxAdd];
+};
+
+// For each listed root j in order: bc[v] += mult_j * delta_j[v] (v != root_j),
+// bc[root_j] += root_add_j.
+__global__ void k_add_scaled(uint32_t n, double *__restrict__ bc, const double *__restrict__ delta, AddList l) {
     const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n) return;
-    bc[v] += (v == root) ? root_add : mult * delta[v];
+    double acc = bc[v];
+    for (uint32_t j = 0; j < l.count; ++j)
+        acc += (v == l.root[j]) ? l.root_add[j] : l.mult[j] * delta[(size_t)l.slot[j] * n + v];
+    bc[v] = acc;
 }
 
 int bcg_run_slots(bcg_graph *g, uint32_t width, const uint32_t *roots, uint32_t nroots, double *d_delta,
@@ -1093,8 +1117,8 @@ int bcg_run_slots(bcg_graph *g, uint32_t width, const uint32_t *roots, uint32_t 
     if (!g || (nroots && !roots) || !d_delta) return set_error(BCG_ERR_ARG, "null argument");
     if (g->trees) return set_error(BCG_ERR_ARG, "graph was created with BCG_PRUNE_TREES");
     if (width != 1 && width != 3 && width != 6) return set_error(BCG_ERR_ARG, "batch width %u not in {1,3,6}", width);
-    if (nroots == 0 || nroots > width) return set_error(BCG_ERR_ARG, "%u roots for a batch of width %u", nroots, width);
-    const size_t n = g->n, cells = n * width;
+    if (nroots == 0) return set_error(BCG_ERR_ARG, "no roots");
+    const size_t n = g->n, cells = n * (((size_t)nroots + width - 1) / width * width);
     RunPlan p;
     for (uint32_t k = 0; k < nroots; ++k) {
         if (roots[k] >= g->n) return set_error(BCG_ERR_ARG, "root %u >= n=%u", roots[k], g->n);
@@ -1104,10 +1128,10 @@ int bcg_run_slots(bcg_graph *g, uint32_t width, const uint32_t *roots, uint32_t 
         p.count.push_back(1);
     }
     if (g->slot_level_cap < cells) {
-        cudaFree(g->d_slot_level);
+        dev_free(g->d_slot_level);
         g->d_slot_level = nullptr;
         g->slot_level_cap = 0;
-        CK(cudaMalloc(&g->d_slot_level, cells * sizeof(int32_t)));
+        CK(dev_alloc(&g->d_slot_level, cells * sizeof(int32_t)));
         g->slot_level_cap = cells;
     }
     CK(cudaMemsetAsync(d_delta, 0, cells * sizeof(double), 0));
@@ -1127,12 +1151,23 @@ int bcg_run_slots(bcg_graph *g, uint32_t width, const uint32_t *roots, uint32_t 
     return BCG_OK;
 }
 
-int bcg_add_scaled(bcg_graph *g, const double *d_delta, double mult, uint32_t root, double root_add) {
+int bcg_add_scaled(bcg_graph *g, const double *d_delta, uint32_t count, const uint32_t *slot, const double *mult,
+                   const uint32_t *root, const double *root_add) {
     clear_error();
-    if (!g || !d_delta) return set_error(BCG_ERR_ARG, "null argument");
-    if (root >= g->n) return set_error(BCG_ERR_ARG, "root %u >= n=%u", root, g->n);
+    if (!g || !d_delta || (count && (!slot || !mult || !root || !root_add))) return set_error(BCG_ERR_ARG, "null argument");
+    if (count > kMaxAdd) return set_error(BCG_ERR_ARG, "%u roots in one call (at most %u)", count, kMaxAdd);
+    if (count == 0) return BCG_OK;
+    AddList l{};
+    l.count = count;
+    for (uint32_t j = 0; j < count; ++j) {
+        if (root[j] >= g->n) return set_error(BCG_ERR_ARG, "root %u >= n=%u", root[j], g->n);
+        l.slot[j] = slot[j];
+        l.root[j] = root[j];
+        l.mult[j] = mult[j];
+        l.root_add[j] = root_add[j];
+    }
     const uint32_t n = g->n;
-    k_add_scaled<<<(n + 255) / 256, 256>>>(n, g->d_bc, d_delta, mult, root, root_add);
+    k_add_scaled<<<(n + 255) / 256, 256>>>(n, g->d_bc, d_delta, l);
     CK(cudaGetLastError());
     return BCG_OK;
 }
@@ -1152,7 +1187,7 @@ int bcg_run_root_levels(bcg_graph *g, uint32_t root, double mult, uint32_t pend,
     p.mult.push_back(mult);
     p.pend.push_back(pend);
     p.count.push_back(1);
-    if (!g->d_level_out) CK(cudaMalloc(&g->d_level_out, (size_t)g->n * sizeof(int32_t)));
+    if (!g->d_level_out) CK(dev_alloc(&g->d_level_out, (size_t)g->n * sizeof(int32_t)));
     DebugOut out;  // width 1, levels only: bc accumulates as in a plain run
     out.width = 1;
     out.level = g->d_level_out;

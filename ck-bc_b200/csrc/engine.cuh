@@ -140,8 +140,8 @@ struct BatchArgs {
     unsigned long long nnz; // adjacency entries of the pruned graph
     float push_pull_ratio;  // pull when frontier pair-edges >= ratio * unvisited pair-edges
     int directed;           // 1: adjacency is not symmetric, pull is not allowed
-    // debug outputs of a single-batch run (nullptr otherwise): slot k of
-    // vertex v at [k * n + v]; levels and sigma are copied after the forward
+    // debug outputs (nullptr otherwise): slot k of batch b, vertex v at
+    // [(b * S + k) * n + v]; levels and sigma are copied after the forward
     // pass, delta is written by the backward pass (which then runs down to
     // level 0)
     int32_t *dbg_level;

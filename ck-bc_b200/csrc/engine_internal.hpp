@@ -90,16 +90,24 @@ struct bcg_graph {
 
 namespace bcg {
 
-// Temporaries of graph creation, from a library-owned stream-ordered pool of
-// the current device that keeps up to 1 GiB reserved once they are freed:
-// creating graphs one after another then neither maps fresh memory nor
-// waits for the device in cudaFree.  Ordered on stream st like a kernel.
+// Device memory of graphs and of their creation, from a library-owned
+// stream-ordered pool of the current device that keeps up to 1 GiB reserved
+// once it is freed: creating and destroying graphs one after another then
+// neither maps fresh memory nor waits in cudaFree.  tmp_alloc / tmp_free are
+// ordered on stream st like a kernel; dev_alloc / dev_free on the default
+// stream.  Whoever frees memory that work on another stream may still use
+// synchronises the device first (graph_free and the reallocating paths do).
 cudaError_t tmp_alloc(void **p, size_t bytes, cudaStream_t st);
 cudaError_t tmp_free(void *p, cudaStream_t st);
 template <class T>
 cudaError_t tmp_alloc(T **p, size_t bytes, cudaStream_t st) {
     return tmp_alloc(reinterpret_cast<void **>(p), bytes, st);
 }
+template <class T>
+cudaError_t dev_alloc(T **p, size_t bytes) {
+    return tmp_alloc(reinterpret_cast<void **>(p), bytes, 0);
+}
+inline cudaError_t dev_free(void *p) { return tmp_free(p, 0); }
 
 // ext: sigma and X as extended-range numbers (ext64.cuh) instead of uint64 / double
 int launch_sweep(int S, const BatchArgs &a, cudaStream_t st, int *grid_out, bool ext = false);

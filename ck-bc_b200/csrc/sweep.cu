@@ -811,7 +811,7 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
                     if (a.slot_delta) a.slot_delta[(size_t)k * a.n + v] = delta;
                     else add += sm.mult[k] * delta;
                 }
-                if (a.dbg_delta) a.dbg_delta[(size_t)k * a.n + v] = delta;
+                if (a.dbg_delta) a.dbg_delta[((size_t)x.b * S + k) * a.n + v] = delta;
             }
             if (d > 0 && !a.slot_delta) {
                 double *bp = a.bc + (a.ext ? a.ext[v] : v);
@@ -1216,8 +1216,9 @@ __global__ void __launch_bounds__(SweepGeom<S>::kThreads, 1) bc_sweep_kernel(Bat
 #pragma unroll
                 for (int k = 0; k < S; ++k) {
                     const uint16_t L = __ldcg(lvl_at(row, k));
-                    if (a.dbg_level) a.dbg_level[(size_t)k * a.n + v] = (L == kUnvisited) ? -1 : (int32_t)L;
-                    if (a.dbg_sigma) a.dbg_sigma[(size_t)k * a.n + v] = (L == kUnvisited) ? 0ull : __ldcg(val_at<S>(row, k));
+                    const size_t o = ((size_t)b * S + k) * a.n + v;  // slot k of batch b
+                    if (a.dbg_level) a.dbg_level[o] = (L == kUnvisited) ? -1 : (int32_t)L;
+                    if (a.dbg_sigma) a.dbg_sigma[o] = (L == kUnvisited) ? 0ull : __ldcg(val_at<S>(row, k));
                 }
             }
             if (!grid_sync(c, nblk, wait_ns)) return;

@@ -412,9 +412,9 @@ __global__ void k_tt_add(uint32_t n, const unsigned long long *__restrict__ acc,
 
 void tree_free(bcg_graph *g) {
     TreeDev &t = g->tdev;
-    cudaFree(t.parent); cudaFree(t.sz); cudaFree(t.comp); cudaFree(t.comp_n); cudaFree(t.order);
-    cudaFree(t.anchor); cudaFree(t.intl); cudaFree(t.cdeg);
-    cudaFree(t.cnt); cudaFree(t.sub); cudaFree(t.csrc); cudaFree(t.acc); cudaFree(t.src); cudaFree(t.info);
+    dev_free(t.parent); dev_free(t.sz); dev_free(t.comp); dev_free(t.comp_n); dev_free(t.order);
+    dev_free(t.anchor); dev_free(t.intl); dev_free(t.cdeg);
+    dev_free(t.cnt); dev_free(t.sub); dev_free(t.csrc); dev_free(t.acc); dev_free(t.src); dev_free(t.info);
     t = TreeDev{};
 }
 
@@ -442,15 +442,15 @@ int prepare_trees(bcg_graph *g, const uint32_t *d_offs0, const uint32_t *d_adj0,
     }
     CKT(tmp_alloc(&deg, nb, st));
     CKT(tmp_alloc(&rem, nb, st));
-    CKT(cudaMalloc(&t.anchor, nb));
+    CKT(dev_alloc(&t.anchor, nb));
     uint32_t *const anchor = t.anchor;
     CKT(tmp_alloc(&cand, nb, st));
     CKT(tmp_alloc(&fa, nb, st));
     CKT(tmp_alloc(&fb, nb, st));
     CKT(tmp_alloc(&ctr, 4 * sizeof(uint32_t), st));
-    CKT(cudaMalloc(&t.parent, nb));
-    CKT(cudaMalloc(&t.sz, nb));
-    CKT(cudaMalloc(&t.order, nb));
+    CKT(dev_alloc(&t.parent, nb));
+    CKT(dev_alloc(&t.sz, nb));
+    CKT(dev_alloc(&t.order, nb));
     CKT(cudaMemset(ctr, 0, 4 * sizeof(uint32_t)));
     // ctr[0]: frontier of the next round, ctr[1]: vertices removed so far
     k_tp_init<<<nblocks(n, 256), 256, 0, st>>>(n, d_offs0, deg, rem, t.parent, t.sz, anchor, fa, ctr);
@@ -477,11 +477,11 @@ int prepare_trees(bcg_graph *g, const uint32_t *d_offs0, const uint32_t *d_adj0,
     }
     CKT(cudaGetLastError());
     // the kept graph, renumbered
-    CKT(cudaMalloc(&t.cdeg, nb));
+    CKT(dev_alloc(&t.cdeg, nb));
     CKT(tmp_alloc(&tmp, nb + 4 * sizeof(uint32_t), st));
-    CKT(cudaMalloc(&t.intl, nb));
+    CKT(dev_alloc(&t.intl, nb));
     uint32_t *const cdeg = t.cdeg, *const intl = t.intl;
-    CKT(cudaMalloc(&g->d_ext, nb));
+    CKT(dev_alloc(&g->d_ext, nb));
     k_tp_cdeg<<<nblocks((uint64_t)n * 32, 256), 256, 0, st>>>(n, d_offs0, d_adj0, rem, cdeg);
     k_tp_flag<<<nblocks(n, 256), 256, 0, st>>>(n, cdeg, tmp);
     CKT(cudaGetLastError());
@@ -494,26 +494,26 @@ int prepare_trees(bcg_graph *g, const uint32_t *d_offs0, const uint32_t *d_adj0,
     k_tp_len<<<nblocks((uint64_t)n + 1, 256), 256, 0, st>>>(n, g->d_ext, cdeg, tmp);
     CKT(cudaGetLastError());
     // offsets with 4 entries of tail padding (the sweep reads 16-byte pieces)
-    CKT(cudaMalloc(&g->d_offs, ((size_t)n + 1 + 4) * sizeof(uint32_t)));
+    CKT(dev_alloc(&g->d_offs, ((size_t)n + 1 + 4) * sizeof(uint32_t)));
     CKT(cudaMemset(g->d_offs + n + 1, 0, 4 * sizeof(uint32_t)));
     rc = scan_exclusive(tmp, g->d_offs, (uint64_t)n + 1, st);
     if (rc) return rc;
     h_offs2.resize((size_t)n + 1);
     CKT(cudaMemcpy(h_offs2.data(), g->d_offs, ((size_t)n + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost));
     const uint64_t nnz2 = h_offs2[n];
-    CKT(cudaMalloc(&g->d_adj, (nnz2 + 4) * sizeof(uint32_t)));
+    CKT(dev_alloc(&g->d_adj, (nnz2 + 4) * sizeof(uint32_t)));
     CKT(cudaMemset(g->d_adj + nnz2, 0, 4 * sizeof(uint32_t)));
     if (nlive)
         k_tp_fill<<<nblocks((uint64_t)nlive * 32, 256), 256, 0, st>>>(nlive, g->d_ext, d_offs0, d_adj0, intl,
                                                                       g->d_offs, g->d_adj);
     CKT(cudaGetLastError());
     // degree/reach words (internal ids), kept for create_common's buffer
-    CKT(cudaMalloc(&g->d_vinfo_trees, (size_t)n * sizeof(uint2)));
+    CKT(dev_alloc(&g->d_vinfo_trees, (size_t)n * sizeof(uint2)));
     k_tp_vinfo<<<nblocks(n, 256), 256, 0, st>>>(n, g->d_ext, cdeg, rem, t.sz, g->d_vinfo_trees);
     // components
     CKT(tmp_alloc(&root, nb, st));
-    CKT(cudaMalloc(&t.comp, nb));
-    CKT(cudaMalloc(&t.comp_n, (size_t)n * sizeof(unsigned long long)));
+    CKT(dev_alloc(&t.comp, nb));
+    CKT(dev_alloc(&t.comp_n, (size_t)n * sizeof(unsigned long long)));
     CKT(cudaMemset(t.comp_n, 0, (size_t)n * sizeof(unsigned long long)));
     k_uf_init<<<nblocks(n, 256), 256, 0, st>>>(n, root);
     if (nlive) {
@@ -543,10 +543,10 @@ int prepare_trees(bcg_graph *g, const uint32_t *d_offs0, const uint32_t *d_adj0,
     k_tp_comp<<<nblocks(n, 256), 256, 0, st>>>(n, anchor, intl, root, t.comp, t.comp_n);
     CKT(cudaGetLastError());
     // per-run scratch of the tree terms
-    CKT(cudaMalloc(&t.cnt, nb));
-    CKT(cudaMalloc(&t.sub, (size_t)n * sizeof(unsigned long long)));
-    CKT(cudaMalloc(&t.csrc, (size_t)n * sizeof(unsigned long long)));
-    CKT(cudaMalloc(&t.acc, (size_t)n * sizeof(unsigned long long)));
+    CKT(dev_alloc(&t.cnt, nb));
+    CKT(dev_alloc(&t.sub, (size_t)n * sizeof(unsigned long long)));
+    CKT(dev_alloc(&t.csrc, (size_t)n * sizeof(unsigned long long)));
+    CKT(dev_alloc(&t.acc, (size_t)n * sizeof(unsigned long long)));
     g->tile_n = nlive ? nlive : 1;
     g->npruned = t.npeeled;
     return BCG_OK;
@@ -558,13 +558,15 @@ int tree_source_info(bcg_graph *g, const uint32_t *src, uint64_t k, std::vector<
     info.resize(k);
     if (k == 0) return BCG_OK;
     if (t.src_cap < k) {
-        cudaFree(t.src);
-        cudaFree(t.info);
+        CKT(cudaDeviceSynchronize());  // earlier runs (any stream) are done with the old buffers
+        dev_free(t.src);
+        dev_free(t.info);
         t.src = nullptr;
         t.info = nullptr;
         t.src_cap = 0;
-        CKT(cudaMalloc(&t.src, k * sizeof(uint32_t)));
-        CKT(cudaMalloc(&t.info, k * sizeof(uint4)));
+        CKT(dev_alloc(&t.src, k * sizeof(uint32_t)));
+        CKT(dev_alloc(&t.info, k * sizeof(uint4)));
+        CKT(cudaDeviceSynchronize());  // ready for stream st
         t.src_cap = k;
     }
     CKT(cudaMemcpyAsync(t.src, src, k * sizeof(uint32_t), cudaMemcpyHostToDevice, st));

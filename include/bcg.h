@@ -239,24 +239,28 @@ int bcg_run_weighted(bcg_graph *g, const uint32_t *roots, const double *mult,
 int bcg_run_root_levels(bcg_graph *g, uint32_t root, double mult, uint32_t pend, int32_t *level,
                         bcg_stats *stats);
 
-/* Searches up to `width` (1, 3 or 6) roots as one batch of the sweep kernel
- * without adding anything to bc: root k's dependencies (delta of every
- * vertex, root included; 0 where not reached) go to the device array
- * d_delta[k * n .. k * n + n), its depths (-1 = not reached) to the host
- * array level[k * n ..] (may be NULL), the vertices it reached to
+/* Searches the nroots roots in batches of `width` (1, 3 or 6) in one launch
+ * of the sweep kernel without adding anything to bc: root k's dependencies
+ * (delta of every vertex, root included; 0 where not reached) go to the
+ * device array d_delta[k * n .. k * n + n), its depths (-1 = not reached) to
+ * the host array level[k * n ..] (may be NULL), the vertices it reached to
  * visited[k] and the sum of (1 + reach) over them to wsum[k] (both may be
- * NULL).  d_delta holds width * n doubles.  Lets a caller that learns its
- * sources one at a time (the reference driver's per-source loop,
- * bc2d.c:1016-1050) search several ahead and commit each with
- * bcg_add_scaled once it is asked for.  Not available with BCG_PRUNE_TREES. */
+ * NULL).  d_delta holds ceil(nroots / width) * width * n doubles.  Lets a
+ * caller that learns its sources one at a time (the reference driver's
+ * per-source loop, bc2d.c:1016-1050) search several ahead and commit each
+ * with bcg_add_scaled once it is asked for.  Not available with
+ * BCG_PRUNE_TREES. */
 int bcg_run_slots(bcg_graph *g, uint32_t width, const uint32_t *roots, uint32_t nroots, double *d_delta,
                   int32_t *level, uint64_t *visited, uint64_t *wsum);
 
-/* bc[v] += mult * d_delta[v] for every v != root, and bc[root] += root_add
- * (device arrays, n entries; queued on the default stream): one root's
- * weighted dependencies and its pendant source term (update_bc,
- * cuda_kernels.cu:263-277). */
-int bcg_add_scaled(bcg_graph *g, const double *d_delta, double mult, uint32_t root, double root_add);
+/* Commits count (<= 64) searched roots into bc, in the order given: for root
+ * j, bc[v] += mult[j] * d_delta[slot[j] * n + v] for every v != root[j], and
+ * bc[root[j]] += root_add[j] (the root's weighted dependencies and its
+ * pendant source term, update_bc, cuda_kernels.cu:263-277).  slot, mult,
+ * root and root_add are host arrays; one kernel, queued on the default
+ * stream. */
+int bcg_add_scaled(bcg_graph *g, const double *d_delta, uint32_t count, const uint32_t *slot, const double *mult,
+                   const uint32_t *root, const double *root_add);
 
 /* Forces the sources-per-batch width (1, 3 or 6; 0 = automatic). */
 int bcg_set_batch_width(bcg_graph *g, uint32_t width);
