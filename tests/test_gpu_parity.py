@@ -251,3 +251,45 @@ def test_every_sweep_pulls_or_pushes(graphs, ratio, monkeypatch):
             G.set_batch_width(width)
             G.run(src)
             assert_bc_close(G.bc(), ref, f"ratio={ratio} width={width}")
+
+
+def test_run_slots_and_add_scaled(graphs):
+    """bcg_run_slots searches roots in batches of a width without touching bc
+    (here 8 roots: two batches of 6); every root's depths and dependencies
+    match the oracle's single-source run.  bcg_add_scaled then commits a list
+    of roots into bc, which must equal the oracle's bc of those sources."""
+    import ctypes
+    import torch
+    offs, adj = graphs["rmat10"]
+    n = len(offs) - 1
+    deg = np.diff(offs)
+    roots = np.array([int(v) for v in np.nonzero(deg)[0][:8]], dtype=np.uint32)
+    nb = (len(roots) + 5) // 6
+    d_delta = torch.zeros(nb * 6 * n, dtype=torch.float64, device="cuda")
+    level = np.empty(len(roots) * n, dtype=np.int32)
+    visited = np.zeros(len(roots), dtype=np.uint64)
+    wsum = np.zeros(len(roots), dtype=np.uint64)
+    L = bcg.lib()
+    with bcg.Graph(offs, adj) as G:
+        rc = L.bcg_run_slots(G.h, 6, roots.ctypes.data_as(bcg._u32p), len(roots), ctypes.c_void_p(d_delta.data_ptr()),
+                             level.ctypes.data_as(ctypes.c_void_p), visited.ctypes.data_as(ctypes.c_void_p),
+                             wsum.ctypes.data_as(ctypes.c_void_p))
+        assert rc == 0, bcg.lib().bcg_last_error()
+        assert not G.bc().any()
+        dl = d_delta.cpu().numpy()
+        for k, r in enumerate(roots):
+            olvl, osig, odl, _ = oracle.single_source(offs, adj, int(r))
+            assert np.array_equal(level[k * n:(k + 1) * n], olvl), int(r)
+            assert_bc_close(dl[k * n:(k + 1) * n], odl, f"slot delta root={r}")
+            assert visited[k] == np.count_nonzero(olvl >= 0)
+            assert wsum[k] == visited[k]  # no pruning: every reached vertex weighs 1
+        count = 5
+        slot = np.arange(count, dtype=np.uint32)
+        mult = np.ones(count)
+        root_add = np.zeros(count)
+        rc = L.bcg_add_scaled(G.h, ctypes.c_void_p(d_delta.data_ptr()), count, slot.ctypes.data_as(bcg._u32p),
+                              mult.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), roots.ctypes.data_as(bcg._u32p),
+                              root_add.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        assert rc == 0, bcg.lib().bcg_last_error()
+        ref, _ = oracle.bc(offs, adj, roots[:count])
+        assert_bc_close(G.bc(), ref, "committed roots")
