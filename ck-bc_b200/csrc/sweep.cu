@@ -609,24 +609,36 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
     for (int k = 0; k < S; ++k) ls[k] = 0ull;
     // the lane's own vertex: its segments and the running fold of their sums
     const uint32_t myp0 = incl - nseg, myp1 = incl;
-    for (uint32_t r0 = s0; r0 < s1; r0 += 32) {
-        const uint32_t seg = r0 + lane;
-        const bool has = seg < s1;
-        uint32_t j = 0, cnt = 0, e0 = 0, jm = 0;
-        if (has) {
-            j = solo ? 0u : ws.sown[seg];
-            const uint4 vm = ws.vmeta[j];
-            const uint32_t rr = (seg - vm.x) * kItems;
-            cnt = min((uint32_t)kItems, vm.z - rr);
-            e0 = vm.y + rr;
-            jm = vm.w;
-        }
-        uint32_t uu[kItems];
+    if (MODE == kFwdPush) {
+        // Pushes add integers with atomics, so their order is free: the part's
+        // (segment, edge) pairs are spread over all lanes, K = ceil(pairs /
+        // 32) <= kItems consecutive pairs per lane and round, so a sparse part
+        // keeps every lane busy with one edge instead of a few lanes with a
+        // whole segment each.
+        constexpr int NL = RowGeom<S>::kLvlBytes / 4;
+        const uint32_t np = (uint32_t)kItems * (s1 - s0);
+        const uint32_t K = min((uint32_t)kItems, (np + 31u) / 32u);
+        for (uint32_t p0 = 0; p0 < np; p0 += 32u * K) {
+            uint32_t uu[kItems], jq[kItems], jmq[kItems];
 #pragma unroll
-        for (int q = 0; q < kItems; ++q) uu[q] = ((uint32_t)q < cnt && jm) ? adjs[e0 + q] : kSkipItem;
-        if (MODE == kFwdPush) {
+            for (int q = 0; q < kItems; ++q) {
+                uu[q] = kSkipItem;
+                jq[q] = 0;
+                jmq[q] = 0;
+                const uint32_t pp = p0 + lane * K + (uint32_t)q;
+                if ((uint32_t)q < K && pp < np) {
+                    const uint32_t seg = s0 + pp / kItems;
+                    const uint32_t j = solo ? 0u : ws.sown[seg];
+                    const uint4 vm = ws.vmeta[j];
+                    const uint32_t rr = (seg - vm.x) * kItems + pp % kItems;
+                    if (rr < vm.z && vm.w) {
+                        uu[q] = adjs[vm.y + rr];
+                        jq[q] = j;
+                        jmq[q] = vm.w;
+                    }
+                }
+            }
             // the targets' level blocks, then claim / add with atomics
-            constexpr int NL = RowGeom<S>::kLvlBytes / 4;
             LaneCounts<S> lc;
             uint32_t lw[kItems][NL];
 #pragma unroll
@@ -636,7 +648,7 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
             for (int q = 0; q < kItems; ++q) {
                 uint32_t app = kNoTile;
                 if (uu[q] != kSkipItem) {
-                    const uint32_t wv = uu[q];
+                    const uint32_t wv = uu[q], jm = jmq[q];
                     unsigned char *wrow = row_of<S>(a, wv);
                     bool claimed_any = false;
 #pragma unroll
@@ -655,14 +667,33 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
                                 take = (old == (uint16_t)(d + 1));
                             }
                         }
-                        if (take) sigma_atomic<EXT>(val_at<S>(wrow, k), ws.own[j][k], a);
+                        if (take) sigma_atomic<EXT>(val_at<S>(wrow, k), ws.own[jq[q]][k], a);
                     }
                     if (claimed_any) app = claim_tile(a, wv, x.key_next);
                 }
                 append_level<S>(a, ws, app, x);
             }
             flush_counts<S>(ws, lc);
-        } else {
+        }
+        __syncwarp();
+        return;
+    }
+    for (uint32_t r0 = s0; r0 < s1; r0 += 32) {
+        const uint32_t seg = r0 + lane;
+        const bool has = seg < s1;
+        uint32_t j = 0, cnt = 0, e0 = 0, jm = 0;
+        if (has) {
+            j = solo ? 0u : ws.sown[seg];
+            const uint4 vm = ws.vmeta[j];
+            const uint32_t rr = (seg - vm.x) * kItems;
+            cnt = min((uint32_t)kItems, vm.z - rr);
+            e0 = vm.y + rr;
+            jm = vm.w;
+        }
+        uint32_t uu[kItems];
+#pragma unroll
+        for (int q = 0; q < kItems; ++q) uu[q] = ((uint32_t)q < cnt && jm) ? adjs[e0 + q] : kSkipItem;
+        {
             // gather the neighbours' rows (kHalf at a time: all 8 for rows of
             // up to 32 bytes, 4 for 64-byte rows) and sum the matching values
             // in adjacency order
