@@ -619,12 +619,11 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
         const uint32_t np = (uint32_t)kItems * (s1 - s0);
         const uint32_t K = min((uint32_t)kItems, (np + 31u) / 32u);
         for (uint32_t p0 = 0; p0 < np; p0 += 32u * K) {
-            uint32_t uu[kItems], jq[kItems], jmq[kItems];
+            uint32_t uu[kItems], jq[kItems];
 #pragma unroll
             for (int q = 0; q < kItems; ++q) {
                 uu[q] = kSkipItem;
                 jq[q] = 0;
-                jmq[q] = 0;
                 const uint32_t pp = p0 + lane * K + (uint32_t)q;
                 if ((uint32_t)q < K && pp < np) {
                     const uint32_t seg = s0 + pp / kItems;
@@ -634,7 +633,6 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
                     if (rr < vm.z && vm.w) {
                         uu[q] = adjs[vm.y + rr];
                         jq[q] = j;
-                        jmq[q] = vm.w;
                     }
                 }
             }
@@ -648,7 +646,7 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
             for (int q = 0; q < kItems; ++q) {
                 uint32_t app = kNoTile;
                 if (uu[q] != kSkipItem) {
-                    const uint32_t wv = uu[q], jm = jmq[q];
+                    const uint32_t wv = uu[q], jm = ws.vmeta[jq[q]].w;
                     unsigned char *wrow = row_of<S>(a, wv);
                     bool claimed_any = false;
 #pragma unroll
@@ -675,10 +673,9 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
             }
             flush_counts<S>(ws, lc);
         }
-        __syncwarp();
-        return;
     }
-    for (uint32_t r0 = s0; r0 < s1; r0 += 32) {
+    // (push parts were done above)
+    for (uint32_t r0 = s0; MODE != kFwdPush && r0 < s1; r0 += 32) {
         const uint32_t seg = r0 + lane;
         const bool has = seg < s1;
         uint32_t j = 0, cnt = 0, e0 = 0, jm = 0;
