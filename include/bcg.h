@@ -148,7 +148,10 @@ int bcg_graph_create_device(const uint32_t *d_offsets, const uint32_t *d_adj,
                             uint32_t n, uint64_t nnz, uint32_t flags,
                             bcg_graph **out);
 
-/* Frees every device buffer of the graph (fincuda cuda_kernels.cu:1201-1232). */
+/* Frees every device buffer of the graph (fincuda cuda_kernels.cu:1201-1232)
+ * after the device has finished all queued work.  Graph buffers come from a
+ * stream-ordered memory pool of the library (one per device) that keeps up
+ * to 1 GiB reserved once freed, so the next creation reuses the memory. */
 int bcg_graph_destroy(bcg_graph *g);
 
 /* Sets every bc value of the graph to 0. */
