@@ -51,60 +51,8 @@ namespace bcg {
     } while (0)
 
 // ---------------------------------------------------------------------------
-// Pruning kernels.
+// Degree words of an unpruned graph.
 // ---------------------------------------------------------------------------
-
-__global__ void k_prune_mark(uint32_t n, const uint32_t *__restrict__ offs, const uint32_t *__restrict__ adj,
-                             uint32_t *__restrict__ anchor, uint32_t *__restrict__ reach) {
-    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= n) return;
-    uint32_t anc = v;
-    if (offs[v + 1] - offs[v] == 1) {
-        const uint32_t a = adj[offs[v]];
-        const bool pair = (offs[a + 1] - offs[a] == 1);
-        if (!(pair && v < a)) {
-            anc = a;
-            atomicAdd(reach + a, 1u);
-        }
-    }
-    anchor[v] = anc;
-}
-
-// One warp per vertex: drop folded neighbours from the list (order kept).
-__global__ void k_prune_compact(uint32_t n, const uint32_t *__restrict__ offs, uint32_t *__restrict__ adj,
-                                const uint32_t *__restrict__ anchor, const uint32_t *__restrict__ reach,
-                                uint2 *__restrict__ vinfo) {
-    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t lane = threadIdx.x & 31;
-    if (warp >= n) return;
-    const uint32_t v = warp;
-    const uint32_t b = offs[v], e = offs[v + 1];
-    const uint32_t r = reach[v];
-    if (anchor[v] != v) {
-        if (lane == 0) vinfo[v] = make_uint2(0u, 0u);
-        return;
-    }
-    if (r == 0) {
-        if (lane == 0) vinfo[v] = make_uint2(e - b, 0u);
-        return;
-    }
-    uint32_t out = b;
-    for (uint32_t base = b; base < e; base += 32) {
-        const uint32_t i = base + lane;
-        uint32_t w = 0;
-        bool keep = false;
-        if (i < e) {
-            w = adj[i];
-            keep = (anchor[w] == w);
-        }
-        const unsigned bal = __ballot_sync(0xffffffffu, keep);
-        __syncwarp();
-        if (keep) adj[out + __popc(bal & ((1u << lane) - 1u))] = w;
-        out += __popc(bal);
-        __syncwarp();
-    }
-    if (lane == 0) vinfo[v] = make_uint2(out - b, r);
-}
 
 __global__ void k_vinfo_plain(uint32_t n, const uint32_t *__restrict__ offs, uint2 *__restrict__ vinfo) {
     const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
@@ -219,7 +167,7 @@ static void graph_free(bcg_graph *g) {
     if (cur != g->device) cudaSetDevice(g->device);
     cudaDeviceSynchronize();  // work on any stream may still read the buffers
     dev_free(g->d_offs); dev_free(g->d_adj); dev_free(g->d_vinfo);
-    dev_free(g->d_anchor); dev_free(g->d_reach); dev_free(g->d_bc);
+    dev_free(g->d_bc);
     dev_free(g->d_tiles); dev_free(g->d_hub_acc); dev_free(g->d_hub_cnt);
     dev_free(g->d_tile_of); dev_free(g->d_tmark); dev_free(g->d_lists);
     dev_free(g->d_lbase); dev_free(g->d_lcnt); dev_free(g->d_ulist); dev_free(g->d_bc_save);
@@ -328,29 +276,11 @@ static int create_common(bcg_graph *g, const uint32_t *h_offs, const uint32_t *h
     uint32_t *hd = g->h_deg.data();
 #pragma omp parallel for schedule(static)
     for (int64_t v = 0; v < (int64_t)n; ++v) hd[v] = h_offs_in[v + 1] - h_offs_in[v];
-    const bool prune = (g->flags & BCG_PRUNE_DEGREE1) && !(g->flags & BCG_DIRECTED);
-    const unsigned nb = (n + 255) / 256;
-    if (prune) {
-        CK(dev_alloc(&g->d_anchor, (size_t)n * sizeof(uint32_t)));
-        CK(dev_alloc(&g->d_reach, (size_t)n * sizeof(uint32_t)));
-        CK(cudaMemset(g->d_reach, 0, (size_t)n * sizeof(uint32_t)));
-        k_prune_mark<<<nb, 256>>>(n, g->d_offs, g->d_adj, g->d_anchor, g->d_reach);
-        CK(cudaGetLastError());
-        const uint64_t threads = (uint64_t)n * 32;
-        k_prune_compact<<<(unsigned)((threads + 255) / 256), 256>>>(n, g->d_offs, g->d_adj, g->d_anchor,
-                                                                    g->d_reach, g->d_vinfo);
-        CK(cudaGetLastError());
-        g->h_anchor.resize(n);
-        CK(cudaMemcpy(g->h_anchor.data(), g->d_anchor, (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-        uint32_t np = 0;
-        for (uint32_t v = 0; v < n; ++v) np += (g->h_anchor[v] != v);
-        g->npruned = np;
-        g->nnz_pruned = g->nnz - 2ull * np;
-    } else {
-        k_vinfo_plain<<<nb, 256>>>(n, g->d_offs, g->d_vinfo);
-        CK(cudaGetLastError());
-        g->nnz_pruned = g->nnz;
-    }
+    // a pruned graph's degree words come from the peeling (graph_create_impl
+    // copies them over these)
+    k_vinfo_plain<<<(n + 255) / 256, 256>>>(n, g->d_offs, g->d_vinfo);
+    CK(cudaGetLastError());
+    g->nnz_pruned = g->nnz;
     CK(dev_alloc(&g->d_lbase, (size_t)(kMaxLevel + 3) * sizeof(uint32_t)));
     CK(dev_alloc(&g->d_lcnt, (size_t)(kMaxLevel + 3) * sizeof(uint32_t)));
     const int rc = setup_tiles(g, h_offs);
@@ -406,12 +336,12 @@ struct RunPlan {
     std::vector<double> mult;
     std::vector<uint64_t> count;  // sources mapped to each root
     uint64_t skipped = 0;
-    // trees mode: sources in components that are trees (no search needed)
+    // pruned: sources in components that are trees (no search needed)
     uint64_t tree_only = 0, tree_edges = 0, tree_verts = 0;
     uint64_t launches = 0;  // kernels the planning launched (the source gather)
 };
 
-// Trees mode: the closed-form bc of the tree vertices (and the anchors' tree
+// A pruned graph: the closed-form bc of the tree vertices (and the anchors' tree
 // terms) for this run's sources, added on the device after the search.
 static int add_tree_terms(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_stats *stats) {
     uint64_t nl = 0;
@@ -425,7 +355,7 @@ static int add_tree_terms(bcg_graph *g, const RunPlan &p, cudaStream_t st, bcg_s
     return BCG_OK;
 }
 
-// Trees mode reads each source's anchor words from the device first
+// A pruned graph reads each source's anchor words from the device first
 // (tree_source_info on stream st), which also leaves the sources there for
 // the tree terms.
 static int plan_run(bcg_graph *g, const uint32_t *src, uint64_t nsrc, RunPlan &p, cudaStream_t st) {
@@ -456,8 +386,6 @@ static int plan_run(bcg_graph *g, const uint32_t *src, uint64_t nsrc, RunPlan &p
             }
             r = w.x;
             root = w.z;
-        } else if (!g->h_anchor.empty()) {
-            r = root = g->h_anchor[s];
         }
         auto it = idx.find(r);
         uint32_t k;
@@ -473,7 +401,6 @@ static int plan_run(bcg_graph *g, const uint32_t *src, uint64_t nsrc, RunPlan &p
         }
         p.mult[k] += 1.0;
         p.count[k] += 1;
-        if (r != s && !g->trees) p.pend[k] += 1;
     }
     return BCG_OK;
 }
@@ -745,10 +672,12 @@ static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint3
         rc = validate_csr(offsets, adj, n, nnz);
         if (rc) return rc;
     }
-    // iterated pendant-tree pruning: the device peels the trees and keeps
-    // the kept graph only
-    const bool trees = (flags & BCG_PRUNE_TREES) && !(flags & BCG_DIRECTED);
-    if (trees) flags &= ~BCG_PRUNE_DEGREE1;
+    // pendant pruning: the device peels the trees (BCG_PRUNE_TREES) or one
+    // layer of degree-1 vertices (BCG_PRUNE_DEGREE1: one peeling round) and
+    // keeps the kept graph only, renumbered
+    const bool trees = (flags & (BCG_PRUNE_TREES | BCG_PRUNE_DEGREE1)) && !(flags & BCG_DIRECTED);
+    const uint32_t max_rounds = (flags & BCG_PRUNE_TREES) ? 0xFFFFFFFFu : 1u;
+    if (flags & BCG_PRUNE_TREES) flags &= ~BCG_PRUNE_DEGREE1;
     bcg_graph *g = new bcg_graph();
     cudaGetDevice(&g->device);
     g->n = n;
@@ -784,7 +713,7 @@ static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint3
             d_offs0 = t_offs;
             d_adj0 = t_adj;
         }
-        rc = prepare_trees(g, d_offs0, d_adj0, nnz, device_in, h_offs2);
+        rc = prepare_trees(g, d_offs0, d_adj0, nnz, device_in, max_rounds, h_offs2);
         drop();
         if (rc) return fail(rc);
         g->nnz = h_offs2[n];  // kept entries, while the common setup runs
@@ -905,8 +834,8 @@ int bcg_bc_csr(const uint32_t *offsets, const uint32_t *adj, uint32_t n, uint64_
 // One batch of up to `width` roots (caller's ids) run in debug mode: every
 // slot's levels and sigma after the forward pass and delta after the
 // backward pass, copied out slot-major in the caller's numbering (nroots * n
-// values each; vertices the search does not hold, i.e. pendant-tree
-// vertices in BCG_PRUNE_TREES mode, read level -1, sigma 0, delta 0).  The bc
+// values each; vertices the search does not hold, i.e. the folded vertices
+// of a pruned graph, read level -1, sigma 0, delta 0).  The bc
 // accumulator is saved and restored around the run.
 static int debug_batch_impl(bcg_graph *g, uint32_t width, const uint32_t *roots, uint32_t nroots, int32_t *level,
                             uint64_t *sigma, double *delta) {
@@ -919,7 +848,7 @@ static int debug_batch_impl(bcg_graph *g, uint32_t width, const uint32_t *roots,
     for (uint32_t k = 0; k < nroots; ++k)
         if (roots[k] >= g->n) return set_error(BCG_ERR_ARG, "root %u >= n=%u", roots[k], g->n);
     std::vector<uint4> info;
-    std::vector<uint32_t> intl;  // trees mode: caller's id -> internal id
+    std::vector<uint32_t> intl;  // pruned: caller's id -> internal id
     if (g->trees) {
         int rc = tree_source_info(g, roots, nroots, info, 0);
         if (rc) return rc;
@@ -990,7 +919,7 @@ static int debug_batch_impl(bcg_graph *g, uint32_t width, const uint32_t *roots,
 }
 
 static int single_source_impl(bcg_graph *g, uint32_t src, int32_t *level, uint64_t *sigma, double *delta) {
-    if (g->trees) return set_error(BCG_ERR_ARG, "single-source runs are not available with BCG_PRUNE_TREES");
+    if (g->trees) return set_error(BCG_ERR_ARG, "single-source runs are not available on a pruned graph");
     if (src >= g->n) return set_error(BCG_ERR_ARG, "source %u >= n=%u", src, g->n);
     return debug_batch_impl(g, 1, &src, 1, level, sigma, delta);
 }
@@ -1040,12 +969,17 @@ int bcg_graph_pruning(bcg_graph *g, uint32_t *anchor, uint32_t *reach) {
     const size_t n = g->n;
     if (anchor) {
         if (g->trees) CK(cudaMemcpy(anchor, g->tdev.anchor, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-        else if (g->h_anchor.empty()) for (size_t v = 0; v < n; ++v) anchor[v] = (uint32_t)v;
-        else memcpy(anchor, g->h_anchor.data(), n * sizeof(uint32_t));
+        else for (size_t v = 0; v < n; ++v) anchor[v] = (uint32_t)v;
     }
     if (reach) {
-        if (!g->d_reach) memset(reach, 0, n * sizeof(uint32_t));
-        else CK(cudaMemcpy(reach, g->d_reach, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        memset(reach, 0, n * sizeof(uint32_t));
+        if (g->trees) {
+            // a kept vertex's subtree size less itself; peeled vertices 0
+            std::vector<uint32_t> anc(n);
+            CK(cudaMemcpy(anc.data(), g->tdev.anchor, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(reach, g->tdev.sz, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+            for (size_t v = 0; v < n; ++v) reach[v] = anc[v] == v ? reach[v] - 1u : 0u;
+        }
     }
     return BCG_OK;
 }
@@ -1063,8 +997,7 @@ int bcg_graph_info(bcg_graph *g, uint32_t *n, uint64_t *nnz, uint64_t *nnz_prune
 int bcg_graph_set_reach(bcg_graph *g, const uint32_t *reach) {
     clear_error();
     if (!g || !reach) return set_error(BCG_ERR_ARG, "null argument");
-    if (g->trees) return set_error(BCG_ERR_ARG, "graph was created with BCG_PRUNE_TREES");
-    if (g->flags & BCG_PRUNE_DEGREE1) return set_error(BCG_ERR_ARG, "graph was created with BCG_PRUNE_DEGREE1");
+    if (g->trees) return set_error(BCG_ERR_ARG, "graph was created with a pruning flag");
     const size_t n = g->n;
     std::vector<uint2> vi(n);
     for (size_t v = 0; v < n; ++v) vi[v] = make_uint2(g->h_deg[v], reach[v]);
@@ -1076,7 +1009,7 @@ int bcg_run_weighted(bcg_graph *g, const uint32_t *roots, const double *mult, co
                      uint64_t nroots, bcg_stats *stats) {
     clear_error();
     if (!g || (nroots && (!roots || !mult))) return set_error(BCG_ERR_ARG, "null argument");
-    if (g->trees) return set_error(BCG_ERR_ARG, "graph was created with BCG_PRUNE_TREES");
+    if (g->trees) return set_error(BCG_ERR_ARG, "graph was created with a pruning flag");
     bcg_stats local{};
     bcg_stats *st = stats ? stats : &local;
     *st = bcg_stats{};
@@ -1115,7 +1048,7 @@ int bcg_run_slots(bcg_graph *g, uint32_t width, const uint32_t *roots, uint32_t 
                   int32_t *level, uint64_t *visited, uint64_t *wsum) {
     clear_error();
     if (!g || (nroots && !roots) || !d_delta) return set_error(BCG_ERR_ARG, "null argument");
-    if (g->trees) return set_error(BCG_ERR_ARG, "graph was created with BCG_PRUNE_TREES");
+    if (g->trees) return set_error(BCG_ERR_ARG, "graph was created with a pruning flag");
     if (width != 1 && width != 3 && width != 6) return set_error(BCG_ERR_ARG, "batch width %u not in {1,3,6}", width);
     if (nroots == 0) return set_error(BCG_ERR_ARG, "no roots");
     const size_t n = g->n, cells = n * (((size_t)nroots + width - 1) / width * width);
@@ -1176,7 +1109,7 @@ int bcg_run_root_levels(bcg_graph *g, uint32_t root, double mult, uint32_t pend,
                         bcg_stats *stats) {
     clear_error();
     if (!g || !level) return set_error(BCG_ERR_ARG, "null argument");
-    if (g->trees) return set_error(BCG_ERR_ARG, "graph was created with BCG_PRUNE_TREES");
+    if (g->trees) return set_error(BCG_ERR_ARG, "graph was created with a pruning flag");
     if (root >= g->n) return set_error(BCG_ERR_ARG, "root %u >= n=%u", root, g->n);
     bcg_stats local{};
     bcg_stats *st = stats ? stats : &local;

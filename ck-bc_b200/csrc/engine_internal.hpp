@@ -16,8 +16,8 @@ using bcg::kTileEdges;
 using bcg::kTileVerts;
 
 namespace bcg {
-// Pendant trees of a graph on the device (BCG_PRUNE_TREES; trees_gpu.cu),
-// caller's numbering.
+// Pendant trees of a graph on the device (BCG_PRUNE_TREES, and one peeling
+// round for BCG_PRUNE_DEGREE1; trees_gpu.cu), caller's numbering.
 struct TreeDev {
     uint32_t *parent = nullptr;  // vertex it hung from when peeled; kNoRoot for kept vertices
     uint32_t *sz = nullptr;      // vertices in the subtree (a kept vertex: 1 + its trees)
@@ -47,7 +47,6 @@ struct bcg_graph {
     uint32_t npruned = 0;
     uint32_t *d_offs = nullptr, *d_adj = nullptr;
     uint2 *d_vinfo = nullptr;
-    uint32_t *d_anchor = nullptr, *d_reach = nullptr;
     double *d_bc = nullptr;
     Tile *d_tiles = nullptr;
     uint32_t ntiles = 0, nhub = 0, nhubchunks = 0;
@@ -65,18 +64,17 @@ struct bcg_graph {
     RootStat *d_rstat = nullptr;
     size_t run_cap = 0;
     std::vector<uint32_t> h_deg;     // original degree (source skip test)
-    std::vector<uint32_t> h_anchor;  // empty when not pruned
     uint32_t forced_width = 0;
     uint32_t tile_vcap = kTileVerts, tile_ecap = kTileEdges;  // tile shape (autotuned by batches)
     std::vector<uint32_t> tile_breaks;  // sorted vertices where a new tile must start
     float ratio = 0.2f;
-    bool trees = false;               // BCG_PRUNE_TREES: pendant trees folded (tdev)
+    bool trees = false;               // pruned: pendant trees (or one layer) folded (tdev)
     bcg::TreeDev tdev;
     uint2 *d_vinfo_trees = nullptr;   // degree/reach words built by the peeling (until creation ends)
     int32_t *d_level_out = nullptr;   // depths exported by bcg_run_root_levels
     int32_t *d_slot_level = nullptr;  // depths exported by bcg_run_slots (width * n)
     size_t slot_level_cap = 0;
-    // Trees mode numbers the searched vertices internally: the vertices with
+    // A pruned graph numbers the searched vertices internally: the vertices with
     // kept edges first (caller's order), then the rest, so the tiles cover
     // [0, tile_n) only.  tdev.intl: caller's id -> internal id; d_ext:
     // internal id -> caller's id, where the sweep adds each vertex's bc.
@@ -135,12 +133,13 @@ int check_ctrl(bcg_graph *g, cudaStream_t st);
 // Rebuilds the work tiles with another shape (vcap vertices, ecap entries).
 int graph_retile(bcg_graph *g, uint32_t vcap, uint32_t ecap, bool force = false);
 // Peels the pendant trees of the input CSR (device arrays d_offs0 / d_adj0,
-// nnz entries; check_ids: verify every id < n first) and builds g's kept
+// nnz entries; check_ids: verify every id < n first; at most max_rounds
+// peeling rounds, 1 for the one-layer mode) and builds g's kept
 // graph in internal numbering (d_offs, d_adj, d_ext, tile_n, degree/reach
 // words in d_vinfo_trees) and the tree arrays (tdev).  h_offs2: the kept
 // graph's offsets.
 int prepare_trees(bcg_graph *g, const uint32_t *d_offs0, const uint32_t *d_adj0, uint64_t nnz, bool check_ids,
-                  std::vector<uint32_t> &h_offs2);
+                  uint32_t max_rounds, std::vector<uint32_t> &h_offs2);
 // Uploads the k sources src (caller's ids, all < n) and reads back, per
 // source s, {anchor a of s, kept degree of a, internal id of a, tree size of
 // a}; the sources stay on the device for tree_terms.  Synchronises st.

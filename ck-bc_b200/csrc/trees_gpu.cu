@@ -3,7 +3,10 @@
 // (degree_reduction, bc2d.c:314-419, then init_bc_1degree / init_delta,
 // bc2d.c:455-465, cuda_kernels.cu:1083-1098); here whole trees hanging off
 // the graph's 2-core are folded, and the betweenness of the tree vertices
-// is computed in closed form.
+// is computed in closed form.  BCG_PRUNE_DEGREE1 is the same machinery
+// stopped after the first round: exactly the reference's one layer (the
+// same vertices fold into the same anchors, by the same pair rule), with the
+// kept graph renumbered like the trees mode's.
 //
 // Peeling runs in rounds.  Round r removes every vertex whose degree among
 // the vertices not yet removed is 1; its one remaining neighbour becomes its
@@ -28,6 +31,8 @@
 //     requested sources in its tree, with weight mult(a) = [a in S] +
 //     (sources in T_a), and every core vertex weighs 1 + reach (its tree's
 //     size - 1) as a target (the engine's reach weights, init_delta).
+// The argument needs only that every removed subtree hangs from the kept
+// graph by one edge, so it holds when peeling stops after any round.
 // Every term is an integer below 2^53, so the device adds them with 64-bit
 // integer atomics: the result does not depend on the order of the adds.
 //
@@ -419,7 +424,7 @@ void tree_free(bcg_graph *g) {
 }
 
 int prepare_trees(bcg_graph *g, const uint32_t *d_offs0, const uint32_t *d_adj0, uint64_t nnz, bool check_ids,
-                  std::vector<uint32_t> &h_offs2) {
+                  uint32_t max_rounds, std::vector<uint32_t> &h_offs2) {
     const uint32_t n = g->n;
     cudaStream_t st = 0;
     TreeDev &t = g->tdev;
@@ -459,7 +464,7 @@ int prepare_trees(bcg_graph *g, const uint32_t *d_offs0, const uint32_t *d_adj0,
     CKT(cudaMemcpy(hc, ctr, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost));
     uint32_t nf = hc[0];
     t.round_off.assign(1, 0);
-    for (uint32_t round = 0; nf; ++round) {
+    for (uint32_t round = 0; nf && round < max_rounds; ++round) {
         CKT(cudaMemset(ctr, 0, sizeof(uint32_t)));
         k_tp_decide<<<nblocks(nf, 256), 256, 0, st>>>(nf, fa, d_offs0, d_adj0, deg, rem, cand);
         k_tp_apply<<<nblocks(nf, 256), 256, 0, st>>>(nf, fa, cand, round, deg, rem, t.parent, t.sz, fb, ctr, t.order,

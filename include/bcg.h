@@ -43,14 +43,17 @@ extern "C" {
 #define BCG_ERR_NOGPU       -9  /* no CUDA device or kernel image for it */
 
 /* flags for bcg_graph_create */
-#define BCG_PRUNE_DEGREE1   0x1u  /* fold degree-1 vertices into their neighbour (bc2d -H 1) */
+#define BCG_PRUNE_DEGREE1   0x1u  /* fold degree-1 vertices into their neighbour (bc2d -H 1):
+                                     one round of BCG_PRUNE_TREES' peeling.  Not available with
+                                     bcg_single_source, bcg_graph_set_reach, bcg_run_weighted,
+                                     bcg_run_root_levels, bcg_run_slots. */
 #define BCG_DIRECTED        0x2u  /* adjacency is not symmetric (bc2d -U): traversal follows
                                      adj[] only; pruning is ignored */
 #define BCG_PRUNE_TREES     0x4u  /* fold whole pendant trees (iterated degree-1 removal), not
                                      just one layer as degree_reduction does (bc2d.c:314-419);
                                      the trees' betweenness is computed in closed form.  Takes
                                      precedence over BCG_PRUNE_DEGREE1.  Not available with
-                                     bcg_single_source, bcg_graph_set_reach, bcg_run_weighted. */
+                                     the calls BCG_PRUNE_DEGREE1 lists. */
 
 /* ---------------------------------------------------------------------------
  * Host-side graph ingest and generation (host code, no GPU needed).
@@ -135,8 +138,8 @@ typedef struct bcg_stats {
 /* Number of CUDA devices visible (0 when none); never fails. */
 int bcg_device_count(void);
 
-/* Uploads a host CSR to the current device and prepares it (degree-1
- * pruning when BCG_PRUNE_DEGREE1 is set, work tiles).  offsets/adj are only
+/* Uploads a host CSR to the current device and prepares it (pendant
+ * pruning on the device when a pruning flag is set, work tiles).  offsets/adj are only
  * read during the call.  Replaces initcuda (cuda_kernels.cu:1123-1198) +
  * init_bc_1degree/init_bc_1degree_device (bc2d.c:455-465,
  * cuda_kernels.cu:1083-1087) + degree_reduction (bc2d.c:314-419). */
@@ -190,9 +193,9 @@ int bcg_bc_csr(const uint32_t *offsets, const uint32_t *adj, uint32_t n,
 /* Single-source detail for parity checks: BFS depth (-1 = unreachable),
  * shortest-path count sigma and dependency delta (delta_s(v) =
  * sum over w with d(w)=d(v)+1 of sigma_v/sigma_w * (1 + delta_w)) of every
- * vertex, for source src on the graph as created (on the pruned graph when
- * it was created with BCG_PRUNE_DEGREE1).  Any output pointer may be NULL.
- * Does not touch the bc accumulator. */
+ * vertex, for source src on the graph as created (BCG_ERR_ARG on a graph
+ * created with a pruning flag: bcg_debug_batch reads pruned graphs).  Any
+ * output pointer may be NULL.  Does not touch the bc accumulator. */
 int bcg_single_source(bcg_graph *g, uint32_t src, int32_t *level,
                       uint64_t *sigma, double *delta);
 
@@ -203,17 +206,18 @@ int bcg_single_source(bcg_graph *g, uint32_t src, int32_t *level,
  * depth (-1 = unreachable), sigma, and delta.  The per-source state the
  * reference keeps in lvl/sig/delta (setcuda + set_mlp_cuda + scan_col_mono2
  * + scan_frt_mono, cuda_kernels.cu:471-599, 689-703, 1100-1119) for `width`
- * sources at once.  Works in every pruning mode: with BCG_PRUNE_TREES the
- * roots must be vertices of the searched 2-core (BCG_ERR_ARG otherwise) and
- * pendant-tree vertices read -1 / 0 / 0.  Exact uint64 counts (overflow is
+ * sources at once.  Works in every pruning mode: on a pruned graph the
+ * roots must be kept vertices with a kept edge (BCG_ERR_ARG otherwise) and
+ * folded vertices read -1 / 0 / 0.  Exact uint64 counts (overflow is
  * BCG_ERR_OVERFLOW).  Does not touch the bc accumulator.  Any output may be
  * NULL. */
 int bcg_debug_batch(bcg_graph *g, uint32_t width, const uint32_t *roots, uint32_t nroots,
                     int32_t *level, uint64_t *sigma, double *delta);
 
-/* Pruning result of a graph created with BCG_PRUNE_DEGREE1: anchor[v] = the
- * vertex v was folded into, or v itself when v was kept; reach[v] = number of
- * vertices folded into v.  Either pointer may be NULL. */
+/* Pruning result of a graph created with a pruning flag: anchor[v] = the
+ * kept vertex v was folded into, or v itself when v was kept; reach[v] =
+ * number of vertices folded into v (0 for folded vertices).  An unpruned
+ * graph reads anchor[v] = v, reach[v] = 0.  Either pointer may be NULL. */
 int bcg_graph_pruning(bcg_graph *g, uint32_t *anchor, uint32_t *reach);
 
 /* Graph sizes after preparation. */
@@ -223,7 +227,7 @@ int bcg_graph_info(bcg_graph *g, uint32_t *n, uint64_t *nnz,
 /* Sets per-vertex pendant weights computed by the caller (the reference's
  * reach[] from its host-side degree_reduction, bc2d.c:314-419 + 455-465,
  * handed over by init_bc_1degree_device, cuda_kernels.cu:1083-1087).  Only
- * for graphs created without BCG_PRUNE_DEGREE1. */
+ * for graphs created without a pruning flag. */
 int bcg_graph_set_reach(bcg_graph *g, const uint32_t *reach);
 
 /* Runs explicit BFS roots with explicit weights: root k's dependencies are
@@ -238,7 +242,8 @@ int bcg_run_weighted(bcg_graph *g, const uint32_t *roots, const double *mult,
  * root's BFS depths level[n] (-1 = unreachable) in the same search: the
  * per-source state the reference's driver reads back between its kernel
  * calls (get_msk and pre_update_bc_cuda after scan_col_csc_cuda_mono,
- * bc2d.c:504-580).  stats may be NULL.  Not available with BCG_PRUNE_TREES. */
+ * bc2d.c:504-580).  stats may be NULL.  Only for graphs created without a
+ * pruning flag. */
 int bcg_run_root_levels(bcg_graph *g, uint32_t root, double mult, uint32_t pend, int32_t *level,
                         bcg_stats *stats);
 
@@ -251,8 +256,8 @@ int bcg_run_root_levels(bcg_graph *g, uint32_t root, double mult, uint32_t pend,
  * NULL).  d_delta holds ceil(nroots / width) * width * n doubles.  Lets a
  * caller that learns its sources one at a time (the reference driver's
  * per-source loop, bc2d.c:1016-1050) search several ahead and commit each
- * with bcg_add_scaled once it is asked for.  Not available with
- * BCG_PRUNE_TREES. */
+ * with bcg_add_scaled once it is asked for.  Only for graphs created
+ * without a pruning flag. */
 int bcg_run_slots(bcg_graph *g, uint32_t width, const uint32_t *roots, uint32_t nroots, double *d_delta,
                   int32_t *level, uint64_t *visited, uint64_t *wsum);
 

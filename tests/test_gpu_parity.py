@@ -127,10 +127,17 @@ def test_pruning_edge_cases():
         with bcg.Graph(offs, adj, bcg.PRUNE_DEGREE1) as G:
             anc, reach = G.pruning()
             assert reach[0] == 3 and anc[1] == 0 and anc[5] == 4 and anc[4] == 4
+            # one layer only: 11 (left with one kept edge) and the path's
+            # middle stay, each holding one folded vertex
+            assert anc[11] == 11 and reach[11] == 1 and anc[12] == 11
+            assert anc[15] == 15 and anc[16] == 16 and reach[15] == reach[16] == 1
+            assert reach[1] == 0 and reach[13] == 0
             st = G.run(src)
             assert_bc_close(G.bc(), ref, f"src={src}")
             assert st.skipped == ost["skipped"]
             assert st.teps_edges == ost["teps_edges"]
+            with pytest.raises(bcg.BcgError):
+                G.single_source(0)  # a pruned graph is renumbered internally
 
 
 def test_hub_chunks_all_modes():

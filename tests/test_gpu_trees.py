@@ -58,6 +58,11 @@ def test_tree_component_and_refusals():
         st = G.run(np.arange(9, dtype=np.uint32))
         assert_bc_close(G.bc(), ref, "path + triangle")
         assert st.teps_edges == ost["teps_edges"]
+        # the path keeps vertex 1 (the last pair resolves to the smaller id);
+        # the tail 7-8 folds into 6
+        anc, reach = G.pruning()
+        assert anc[0] == anc[2] == anc[3] == 1 and anc[7] == anc[8] == 6
+        assert reach[1] == 3 and reach[6] == 2 and reach[4] == 0 and reach[8] == 0
         with pytest.raises(bcg.BcgError):
             G.single_source(0)
         reach = np.zeros(9, dtype=np.uint32)
