@@ -1,4 +1,4 @@
-// Graph handle, degree-1 pruning pre-pass, work tiles and the bcg_* C ABI.
+// Graph handle, work tiles and the bcg_* C ABI.
 //
 // Reference counterparts:
 //   initcuda / fincuda            cuda_kernels.cu:1123-1198, 1201-1232
@@ -7,25 +7,17 @@
 //   per-source loop + skip        bc2d.c:1016-1050
 //   get_bc                        cuda_kernels.cu:1039-1041
 //
-// Degree-1 pruning pre-pass.  A vertex p of degree 1 whose neighbour a
-// does not also have degree 1 is folded into a: p leaves the traversal graph
-// and reach[a] counts it.  For an isolated edge {p, a} (both degree 1) the
-// larger id is folded into the smaller.  The pruned graph keeps the vertex
-// ids and the CSR row starts; each surviving list is compacted to the front of
-// its row and vinfo[v].x holds its new length.  Exact BC is preserved by
-// weighting (Brandes' dependency sum split by which side of the folded edge
-// each endpoint lies on):
-//   - the backward pass starts every delta at reach[v] (init_delta,
-//     cuda_kernels.cu:1089-1098), so pendants count as targets;
-//   - a source s folded into anchor a runs as a BFS from a; the root's
-//     dependencies are added mult(a) = [a requested] + #(requested pendants of
-//     a) times;
-//   - the root gets pend(a) * (W - 2), W = number of original vertices of its
-//     component (update_bc's source term, cuda_kernels.cu:269-271).
-// Unlike the reference, a vertex whose every neighbour was folded (isolated in
-// the pruned graph) is still run as a root, and vertices outside the root's
-// component get nothing (the reference adds reach * (reach_v0 + 1) to them,
-// cuda_kernels.cu:274, 1095).
+// Pendant pruning (both flags) runs on the device in trees_gpu.cu:
+// BCG_PRUNE_DEGREE1 is its first peeling round, which folds exactly the
+// reference's layer: a vertex p of degree 1 whose neighbour a does not also
+// have degree 1 is folded into a, and of an isolated edge {p, a} the larger
+// id is folded into the smaller.  The kept graph is renumbered and searched
+// with reach weights (init_delta, cuda_kernels.cu:1089-1098); the folded
+// vertices' bc and the anchors' terms for their trees are added in closed
+// form.  Unlike the reference, a vertex whose every neighbour was folded
+// (isolated in the pruned graph) still gets its exact bc, and vertices
+// outside a root's component get nothing from it (the reference adds
+// reach * (reach_v0 + 1) to them, cuda_kernels.cu:274, 1095).
 #include <algorithm>
 #include <cinttypes>
 #include <cstdio>
@@ -428,6 +420,7 @@ static void fill_args(bcg_graph *g, BatchArgs &a) {
     a.ctrl = g->d_ctrl;
     a.nnz = g->nnz_pruned;
     a.push_pull_ratio = g->ratio;
+    a.mark_ratio = g->mark_ratio;
     a.directed = (g->flags & BCG_DIRECTED) ? 1 : 0;
 }
 
@@ -684,6 +677,7 @@ static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint3
     g->nnz = nnz;
     g->flags = flags;
     if (const char *e = getenv("BCG_PUSH_PULL_RATIO")) g->ratio = (float)atof(e);
+    if (const char *e = getenv("BCG_CHILD_MARK_RATIO")) g->mark_ratio = (uint32_t)atoi(e);
     if (const char *e = getenv("BCG_TILE_SHAPE")) {  // "<vertices>x<entries>", e.g. 32x128
         unsigned tv = 0, te = 0;
         if (sscanf(e, "%ux%u", &tv, &te) == 2 && tv >= 1 && tv <= (unsigned)kTileVerts && te >= 1 &&

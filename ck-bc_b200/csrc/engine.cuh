@@ -34,7 +34,10 @@ constexpr unsigned long long kDefaultWaitNs = 20ull * 1000 * 1000 * 1000;  // 20
 // of S 16-bit levels padded to 8 bytes (16 for S = 6), then S 64-bit values:
 // 16, 32 or 64 bytes, i.e. half of, one or two 32-byte sectors.  The value of
 // a slot is sigma during the forward pass and (1 + delta) / sigma after the
-// vertex's backward step.
+// vertex's backward step.  The padding of the level block holds the child
+// marks: bit k (from kMarkShift on in word kMarkWord) is cleared once a
+// vertex of level L + 1 in slot k has found the vertex, at level L in slot
+// k, as its parent (the batch reset sets the whole block to ones).
 template <int S>
 struct RowGeom {
     static_assert(S == 1 || S == 3 || S == 6, "batch width must be 1, 3 or 6");
@@ -43,6 +46,12 @@ struct RowGeom {
     static constexpr int kWords = kBytes / 4;
     static constexpr int kVec = kBytes / 16;
     static constexpr int kValWord = kLvlBytes / 4;  // first word of the values
+    // the level block's free halfwords: word 1's upper half (S = 1, 3) or
+    // word 3 (S = 6, the levels of slots 6 and 7 that do not exist)
+    static constexpr int kMarkWord = (S <= 4) ? 1 : 3;
+    static constexpr int kMarkShift = (S <= 4) ? 16 : 0;
+    static_assert(16 * S <= 32 * kMarkWord + kMarkShift && 32 * kMarkWord + kMarkShift + S <= 8 * kLvlBytes,
+                  "marks lie between the levels and the values");
 };
 
 __host__ __device__ constexpr int row_bytes(int S) { return ((S <= 4) ? 8 : 16) + 8 * S; }
@@ -139,6 +148,8 @@ struct BatchArgs {
     RootStat *rstat;        // nbatch * S
     unsigned long long nnz; // adjacency entries of the pruned graph
     float push_pull_ratio;  // pull when frontier pair-edges >= ratio * unvisited pair-edges
+    uint32_t mark_ratio;    // a level marks its parents in the backward pass when its
+                            // pair-edges * mark_ratio < the level above's (0: never)
     int directed;           // 1: adjacency is not symmetric, pull is not allowed
     // debug outputs (nullptr otherwise): slot k of batch b, vertex v at
     // [(b * S + k) * n + v]; levels and sigma are copied after the forward

@@ -68,6 +68,7 @@ struct bcg_graph {
     uint32_t tile_vcap = kTileVerts, tile_ecap = kTileEdges;  // tile shape (autotuned by batches)
     std::vector<uint32_t> tile_breaks;  // sorted vertices where a new tile must start
     float ratio = 0.2f;
+    uint32_t mark_ratio = 8;  // child marks in backward sweeps (BatchArgs::mark_ratio)
     bool trees = false;               // pruned: pendant trees (or one layer) folded (tdev)
     bcg::TreeDev tdev;
     uint2 *d_vinfo_trees = nullptr;   // degree/reach words built by the peeling (until creation ends)

@@ -59,6 +59,17 @@
 // used, so a run's results are bitwise reproducible and a source's
 // contribution does not depend on the batch it shares.
 //
+// Child marks.  A backward sweep at level d reads every edge of every vertex
+// of level d to find its children at level d + 1.  When level d + 1 holds far
+// fewer pair-edges than level d (the last levels of a small-diameter graph),
+// most vertices of level d have no child at all.  So the backward sweep of
+// such a small level d + 1 also marks the parents it sees (level d in the same
+// slot) with an atomic AND on the parent row's mark bits, and the sweep at
+// level d then reads the edges of marked vertices only.  An unmarked vertex
+// has no child in any of its slots: its sums are zero either way, so the
+// results are bitwise the same.  Undirected graphs only (a directed graph's
+// adjacency does not list the parents).
+//
 // Memory coherence.  The L1 caches of the SMs are not coherent with each
 // other: a plain load can hit a line this SM cached in an earlier sweep or
 // batch after another SM rewrote it in L2.  Everything that other SMs rewrite
@@ -261,6 +272,9 @@ struct WarpSmem {
     unsigned long long cnt[2 + 3 * S];
 };
 
+// Levels whose backward sweep may mark parents (a per-CTA bit each).
+constexpr uint32_t kMarkLevels = 2048;
+
 template <int S>
 struct Smem {
     WarpSmem<S> w[SweepGeom<S>::kWarps];
@@ -271,6 +285,7 @@ struct Smem {
     uint32_t roots[S];
     double mult[S];
     uint32_t next;  // work items drawn by this CTA's warps in the current sweep
+    uint32_t mlev[kMarkLevels / 32];  // levels whose backward sweep marks parents
 };
 
 template <int S>
@@ -306,7 +321,10 @@ struct SweepCtx {
     uint32_t next_lvl;   // d + 1 (index into lcnt)
     uint32_t split;      // warps per tile (push sweeps over short lists)
     unsigned long long ubase;  // ring position of this sweep's first unvisited-tile append
+    bool mark;           // backward: mark the parents (level d - 1) of level d's vertices
+    bool filt;           // backward: level d + 1 marked its parents; read marked vertices only
 };
+
 
 __device__ __forceinline__ uint32_t tile_key(uint32_t b, uint32_t level) {
     return ((b & 0xFFFFu) << 16) | (level + 1u);
@@ -570,7 +588,12 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
         if (hub && T.e1 < ee) ee = T.e1;
         if (ee < eb) ee = eb;
         if (m) dg = ee - eb;
-        if (MODE == kBwd && d == x.D) dg = 0;
+        if (MODE == kBwd) {
+            // a vertex with no child in any slot reads no edge (the deepest
+            // level has none), unless its sweep marks parents
+            const uint32_t mk = ~(ow[RowGeom<S>::kMarkWord] >> RowGeom<S>::kMarkShift) & ((1u << S) - 1u);
+            if (!x.mark && (d == x.D || (x.filt && !(m & mk)))) dg = 0;
+        }
         ws.vmeta[lane].y = eb - ab;
         ws.vmeta[lane].z = dg;
         if (MODE == kFwdPush) {
@@ -696,6 +719,7 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
             // in adjacency order
             constexpr int kHalf = (NW <= 8) ? kItems : kItems / 2;
             const uint16_t want = (MODE == kFwdPull) ? dl : (uint16_t)(d + 1);
+            const uint16_t par = (uint16_t)(d - 1);  // parents, in a marking backward sweep
             bool ovf = false;  // a wrapped uint64 sum (flagged once per round)
             auto add = [&](unsigned long long x, unsigned long long y) -> unsigned long long {
                 if (EXT) return ext_add(x, y);
@@ -722,6 +746,19 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
                     for (int k = 0; k < S; ++k) {
                         if (!((jm >> k) & 1u) || w_lvl(wr[q], k) != want) continue;
                         run[k] = add(run[k], w_val<S>(wr[q], k));
+                    }
+                    if (MODE == kBwd && x.mark) {
+                        // the neighbour is a parent in the slots where it sits
+                        // one level up; mark the slots it does not show marked yet
+                        uint32_t pm = 0;
+#pragma unroll
+                        for (int k = 0; k < S; ++k)
+                            pm |= (uint32_t)(((jm >> k) & 1u) && w_lvl(wr[q], k) == par) << k;
+                        pm &= wr[q][RowGeom<S>::kMarkWord] >> RowGeom<S>::kMarkShift;
+                        if (pm)
+                            atomicAnd(reinterpret_cast<unsigned int *>(row_of<S>(a, uu[h0 + q])) +
+                                          RowGeom<S>::kMarkWord,
+                                      ~(pm << RowGeom<S>::kMarkShift));
                     }
                 }
             }
@@ -1044,6 +1081,7 @@ __global__ void __launch_bounds__(SweepGeom<S>::kThreads, 1) bc_sweep_kernel(Bat
             sm.roots[threadIdx.x] = packed ? kNoRoot : a.roots[(size_t)b * S + threadIdx.x];
             sm.mult[threadIdx.x] = packed ? 1.0 : a.mult[(size_t)b * S + threadIdx.x];
         }
+        for (uint32_t i = threadIdx.x; i < kMarkLevels / 32; i += blockDim.x) sm.mlev[i] = 0;
         __syncthreads();
         // frontier / unvisited pair-edge counts of level 0 (same in every CTA)
         unsigned long long pf_cur = 0, pu_cur = 0;
@@ -1172,6 +1210,7 @@ __global__ void __launch_bounds__(SweepGeom<S>::kThreads, 1) bc_sweep_kernel(Bat
             x.key_next = tile_key(b, d + 1);
             x.split = (x.mode == kFwdPush && lc * 2 < total_warps) ? kPushSplit : 1;
             x.ubase = ucur;
+            x.mark = x.filt = false;
             if (threadIdx.x == 0) {
                 sm.next = 0;
                 sm.c_disc = 0; sm.c_pf = 0;
@@ -1225,6 +1264,11 @@ __global__ void __launch_bounds__(SweepGeom<S>::kThreads, 1) bc_sweep_kernel(Bat
                 uall = false;
             }
             if (disc == 0) break;
+            // level d + 1 marks its parents in the backward pass when it holds
+            // far fewer pair-edges than level d (the same decision in every CTA)
+            if (threadIdx.x == 0 && !a.directed && d + 1 >= 2 && d + 1 < kMarkLevels &&
+                pfn * a.mark_ratio < pf_cur)
+                sm.mlev[(d + 1) >> 5] |= 1u << ((d + 1) & 31);
             ++d;
             if (d > kMaxLevel) {
                 if (blockIdx.x == 0 && threadIdx.x == 0) set_error(c, BCG_ERR_DEPTH);
@@ -1267,6 +1311,11 @@ __global__ void __launch_bounds__(SweepGeom<S>::kThreads, 1) bc_sweep_kernel(Bat
             x.lb_next = 0;
             x.next_lvl = 0;
             x.split = 1;
+            auto marks_parents = [&](uint32_t e) {
+                return e < kMarkLevels && ((sm.mlev[e >> 5] >> (e & 31)) & 1u);
+            };
+            x.mark = marks_parents((uint32_t)dd);
+            x.filt = !x.mark && dd >= 1 && marks_parents((uint32_t)dd + 1);
             const uint32_t lb = blb, lc = blc;
             if (dd > lowest) {
                 blb = vload32(a.lbase + dd - 1);
@@ -1276,7 +1325,7 @@ __global__ void __launch_bounds__(SweepGeom<S>::kThreads, 1) bc_sweep_kernel(Bat
             __syncthreads();
             run_sweep<S, EXT>(a, sm, x, a.lists + lb, 0, lc, 0xFFFFFFFFull, pstate, wait_ns);
             if (!grid_sync(c, nblk, wait_ns)) return;
-            trace(a, b, 3u, (uint32_t)dd, lc, 0);
+            trace(a, b, 3u, (uint32_t)dd, lc, (x.mark ? 1u : 0u) | (x.filt ? 2u : 0u));
         }
 
         // ---- served waves: each slot's dependencies into the buffer of the

@@ -69,3 +69,41 @@ def test_source_independent_of_batch_mates(big):
     assert np.array_equal(l3[0], l6[4])
     assert np.array_equal(s3[0], s6[4])
     assert np.array_equal(d3[0].view(np.uint64), d6[4].view(np.uint64))
+
+
+@pytest.mark.parametrize("flags,width,ext", [(bcg.PRUNE_TREES, 6, False), (bcg.PRUNE_DEGREE1, 3, False),
+                                             (0, 1, False), (bcg.PRUNE_TREES, 6, True)])
+def test_child_marks_change_no_bit(big, tmp_path, monkeypatch, flags, width, ext):
+    """Backward sweeps of small levels mark their parents, and the sweep of the
+    level above reads the edges of marked vertices only: the run must mark and
+    filter some levels, and give the same bits as a run without marks (bc, and
+    one batch's delta read-out)."""
+    offs, adj, src = big
+    sample = src[:60]
+    trace = tmp_path / "trace.csv"
+    outs = []
+    for ratio in ("8", "0"):
+        monkeypatch.setenv("BCG_CHILD_MARK_RATIO", ratio)
+        monkeypatch.setenv("BCG_TRACE_FILE", str(trace) if ratio == "8" else "")
+        with bcg.Graph(offs, adj, flags) as G:
+            G.set_batch_width(width)
+            if ext:
+                G.set_sigma_mode(bcg.SIGMA_EXTENDED)
+            G.run(sample)
+            anc, _ = G.pruning()
+            deg_kept = np.zeros(len(anc), dtype=np.int64)
+            kept = anc == np.arange(len(anc), dtype=anc.dtype)
+            np.add.at(deg_kept, np.repeat(np.arange(len(anc)), np.diff(offs))[kept[adj]], 1)
+            roots = [int(s) for s in sample if kept[s] and deg_kept[s] > 0][:width]
+            _, _, dl = G.debug_batch(roots, width)
+            outs.append((G.bc(), dl))
+    flags_seen = set()
+    for line in trace.read_text().splitlines():
+        if line.startswith("#"):
+            continue
+        f = line.split(",")
+        if int(f[1]) == 3:
+            flags_seen.add(int(f[4]))
+    assert 1 in flags_seen and 2 in flags_seen, flags_seen  # some level marked, some filtered
+    assert np.array_equal(outs[0][0].view(np.uint64), outs[1][0].view(np.uint64))
+    assert np.array_equal(outs[0][1].view(np.uint64), outs[1][1].view(np.uint64))
