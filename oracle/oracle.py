@@ -138,9 +138,12 @@ def bc_q(offsets, adj, sources, nthreads: int = 1):
 _TREES = None
 
 
-def peel_trees(offsets, adj):
-    """Host restatement of pendant-tree peeling (trees_ref.cpp) ->
-    (anchor uint32[n], subtree size uint32[n], peeled vertex count)."""
+class TreeStats(ctypes.Structure):
+    _fields_ = [("skipped", ctypes.c_uint64), ("roots", ctypes.c_uint64), ("teps_edges", ctypes.c_uint64),
+                ("peel_seconds", ctypes.c_double), ("overflow", ctypes.c_int)]
+
+
+def _trees_lib():
     global _TREES
     if _TREES is None:
         path = os.path.join(HERE, "libtrees_ref.so")
@@ -149,7 +152,35 @@ def peel_trees(offsets, adj):
         L = ctypes.CDLL(path)
         L.oracle_peel_trees.restype = ctypes.c_int
         L.oracle_peel_trees.argtypes = [ctypes.c_uint32, _u32p, _u32p, _u32p, _u32p, _u64p]
+        L.oracle_bc_trees.restype = ctypes.c_int
+        L.oracle_bc_trees.argtypes = [ctypes.c_uint32, _u32p, _u32p, _u32p, ctypes.c_uint64, ctypes.c_int, _f64p,
+                                      ctypes.POINTER(TreeStats)]
         _TREES = L
+    return _TREES
+
+
+def bc_trees(offsets, adj, sources, nthreads: int = 1):
+    """The same ordered-pair BC sums as bc(), computed with pendant trees
+    folded (trees_ref.cpp: peel, reach-weighted searches of the kept graph
+    from the sources' anchors, closed-form tree terms) -> (bc float64[n],
+    stats dict: skipped, roots, teps_edges, peel_seconds, overflow)."""
+    offsets, adj = _u32(offsets), _u32(adj)
+    s = _u32(sources)
+    n = len(offsets) - 1
+    out = np.zeros(n, np.float64)
+    st = TreeStats()
+    rc = _trees_lib().oracle_bc_trees(n, offsets.ctypes.data_as(_u32p), adj.ctypes.data_as(_u32p),
+                                      s.ctypes.data_as(_u32p), len(s), nthreads, out.ctypes.data_as(_f64p),
+                                      ctypes.byref(st))
+    if rc:
+        raise RuntimeError(f"oracle_bc_trees failed ({rc})")
+    return out, {f: getattr(st, f) for f, _ in st._fields_}
+
+
+def peel_trees(offsets, adj):
+    """Host restatement of pendant-tree peeling (trees_ref.cpp) ->
+    (anchor uint32[n], subtree size uint32[n], peeled vertex count)."""
+    _trees_lib()
     offsets, adj = _u32(offsets), _u32(adj)
     n = len(offsets) - 1
     anc = np.zeros(n, np.uint32)

@@ -24,10 +24,15 @@
 //   - An anchor a gets the same terms for its child subtrees.
 #include <algorithm>
 #include <cstdint>
+#include <chrono>
 #include <deque>
 #include <vector>
 
 #include "trees_ref.hpp"
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 namespace oracle_trees {
 
@@ -186,5 +191,143 @@ extern "C" int oracle_peel_trees(uint32_t n, const uint32_t *offs, const uint32_
         sz[v] = t.sz[v];
     }
     *npeeled = t.order.size();
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Tree-pruned Brandes on the host: the same quantity as oracle_bc, computed the
+// way the engine's BCG_PRUNE_TREES mode does (peel, search the kept graph from
+// every anchor that holds requested sources with reach weights, add the tree
+// terms in closed form).  bench.py times it as the pruned CPU leg beside the
+// unpruned one; tests/test_trees.py pins it to oracle_bc.
+
+namespace oracle_trees {
+
+// One search of the kept graph (internal ids, CSR o2/a2) from root r: every
+// vertex weighs 1 + reach as a target, so delta starts at reach; mult times
+// the dependencies go to acc (the root's own excluded).  lvl must be -1 on
+// entry and is left -1 on exit.  Returns the visited vertices.
+static uint32_t weighted_one(const uint32_t *o2, const uint32_t *a2, const double *reach, uint32_t r, double mult,
+                             int32_t *lvl, uint64_t *sigma, double *delta, uint32_t *queue, double *acc,
+                             int *overflow) {
+    uint32_t head = 0, tail = 0;
+    lvl[r] = 0;
+    sigma[r] = 1;
+    delta[r] = reach[r];
+    queue[tail++] = r;
+    while (head < tail) {
+        const uint32_t c = queue[head++];
+        for (uint32_t e = o2[c]; e < o2[c + 1]; ++e) {
+            const uint32_t w = a2[e];
+            if (lvl[w] < 0) {
+                lvl[w] = lvl[c] + 1;
+                sigma[w] = 0;
+                delta[w] = reach[w];
+                queue[tail++] = w;
+            }
+            if (lvl[w] == lvl[c] + 1) {
+                const uint64_t t = sigma[w] + sigma[c];
+                if (t < sigma[w]) *overflow = 1;
+                sigma[w] = t;
+            }
+        }
+    }
+    // children before parents: walk the queue backwards
+    for (uint32_t i = tail; i-- > 1;) {
+        const uint32_t w = queue[i];
+        const double xw = (1.0 + delta[w]) / (double)sigma[w];
+        for (uint32_t e = o2[w]; e < o2[w + 1]; ++e) {
+            const uint32_t v = a2[e];
+            if (lvl[v] == lvl[w] - 1) delta[v] += (double)sigma[v] * xw;
+        }
+        acc[w] += mult * delta[w];
+    }
+    for (uint32_t i = 0; i < tail; ++i) lvl[queue[i]] = -1;
+    return tail;
+}
+
+}  // namespace oracle_trees
+
+struct oracle_trees_stats {
+    uint64_t skipped;     // sources of degree 0
+    uint64_t roots;       // anchors searched
+    uint64_t teps_edges;  // per source, the edges of its component in the input graph
+    double peel_seconds;  // peeling and component labels
+    int overflow;         // a uint64 path count wrapped
+};
+
+extern "C" int oracle_bc_trees(uint32_t n, const uint32_t *offs, const uint32_t *adj, const uint32_t *sources,
+                               uint64_t nsrc, int nthreads, double *bc, oracle_trees_stats *st) {
+    using namespace oracle_trees;
+    const auto t0 = std::chrono::steady_clock::now();
+    TreeInfo t;
+    std::vector<uint32_t> cdeg, ext, intl, o2, a2;
+    const uint32_t nlive = peel_trees(offs, adj, n, t, cdeg, ext, intl, o2, a2);
+    label_components(o2.data(), a2.data(), n, intl, t);
+    const auto t1 = std::chrono::steady_clock::now();
+    // edges per component of the input graph
+    std::vector<uint64_t> comp_deg(t.comp_n.size(), 0);
+    for (uint32_t v = 0; v < n; ++v) comp_deg[t.comp[v]] += offs[v + 1] - offs[v];
+    // source multiplicities: per vertex (tree terms) and per anchor (searches)
+    std::vector<uint32_t> cnt(n, 0);
+    std::vector<double> mult(nlive, 0.0);
+    uint64_t skipped = 0, teps = 0;
+    for (uint64_t i = 0; i < nsrc; ++i) {
+        const uint32_t s = sources[i];
+        if (s >= n) return -1;
+        if (offs[s + 1] == offs[s]) {
+            ++skipped;
+            continue;
+        }
+        ++cnt[s];
+        teps += comp_deg[t.comp[s]] / 2;
+        const uint32_t ia = intl[t.anchor[s]];
+        if (ia < nlive) mult[ia] += 1.0;  // an anchor with kept edges: searched
+    }
+    std::vector<uint32_t> roots;
+    for (uint32_t i = 0; i < nlive; ++i)
+        if (mult[i] > 0.0) roots.push_back(i);
+    std::vector<double> reach(nlive);
+    for (uint32_t i = 0; i < nlive; ++i) reach[i] = (double)t.sz[ext[i]] - 1.0;
+    int nt = nthreads > 0 ? nthreads : 1;
+#ifndef _OPENMP
+    nt = 1;
+#endif
+    std::vector<double> part((size_t)nt * nlive, 0.0);
+    int overflow = 0;
+#pragma omp parallel num_threads(nt) reduction(| : overflow)
+    {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+        std::vector<int32_t> lvl(nlive, -1);
+        std::vector<uint64_t> sigma(nlive);
+        std::vector<double> delta(nlive);
+        std::vector<uint32_t> queue(nlive);
+        double *acc = part.data() + (size_t)tid * nlive;
+#pragma omp for schedule(dynamic, 1)
+        for (int64_t k = 0; k < (int64_t)roots.size(); ++k) {
+            const uint32_t r = roots[k];
+            weighted_one(o2.data(), a2.data(), reach.data(), r, mult[r], lvl.data(), sigma.data(), delta.data(),
+                         queue.data(), acc, &overflow);
+        }
+    }
+    // thread partials in thread order, then the tree terms
+    for (uint32_t i = 0; i < nlive; ++i) {
+        double s = 0.0;
+        for (int k = 0; k < nt; ++k) s += part[(size_t)k * nlive + i];
+        bc[ext[i]] += s;
+    }
+    std::vector<double> tacc;
+    tree_bc(t, cnt, tacc);
+    for (uint32_t v = 0; v < n; ++v) bc[v] += tacc[v];
+    if (st) {
+        st->skipped = skipped;
+        st->roots = roots.size();
+        st->teps_edges = teps;
+        st->peel_seconds = std::chrono::duration<double>(t1 - t0).count();
+        st->overflow = overflow;
+    }
     return 0;
 }

@@ -199,3 +199,32 @@ def test_parallel_components_match_scipy(tmp_path, spec):
         ref = np.array([first[x] for x in lab])
         assert np.array_equal(comp, ref)
         assert np.array_equal(comp_n, np.bincount(ref, minlength=nref))
+
+
+@pytest.mark.parametrize("spec", ["rmat:scale=10,ef=16,seed=7,pendant_frac=0.1,pendant_mean=4",
+                                  "rmat:scale=11,ef=8,seed=3,pendant_frac=0.3,pendant_mean=6",
+                                  "rmat:scale=9,ef=2,seed=4"])
+def test_pruned_cpu_brandes_matches_oracle(spec):
+    """oracle.bc_trees (peeling, reach-weighted searches of the kept graph from
+    the sources' anchors, closed-form tree terms) against the unpruned
+    Brandes oracle: the same bc, TEPS edges and skipped sources."""
+    offs, adj = bcg.generate(spec)
+    n = len(offs) - 1
+    for src in (np.arange(n, dtype=np.uint32), bcg.sample_sources(n, 90, 5)):
+        ref, ost = oracle.bc(offs, adj, src, nthreads=4)
+        got, st = oracle.bc_trees(offs, adj, src, nthreads=4)
+        assert np.max(np.abs(got - ref) / np.maximum(np.abs(ref), 1.0)) < 1e-12
+        assert st["teps_edges"] == ost["teps_edges"] and st["skipped"] == ost["skipped"]
+
+
+def test_pruned_cpu_brandes_edge_cases():
+    # a star, an isolated edge, a triangle with trees, isolated vertices, a
+    # path; sources repeated, pendant, isolated and in tree components
+    pairs = [[0, 1], [0, 2], [0, 3], [4, 5], [6, 7], [7, 8], [8, 6], [6, 9], [6, 10], [7, 11], [11, 12],
+             [14, 15], [15, 16], [16, 17]]
+    offs, adj = bcg.from_pairs(pairs, 18)
+    for src in (list(range(18)), [1, 1, 2, 5, 9, 12, 13, 14, 14], [13], [3]):
+        ref, ost = oracle.bc(offs, adj, src)
+        got, st = oracle.bc_trees(offs, adj, src)
+        assert np.max(np.abs(got - ref)) < 1e-12, src
+        assert st["teps_edges"] == ost["teps_edges"] and st["skipped"] == ost["skipped"]
