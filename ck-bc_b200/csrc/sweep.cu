@@ -879,8 +879,11 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
                 if (a.dbg_delta) a.dbg_delta[((size_t)x.b * S + k) * a.n + v] = delta;
             }
             if (d > 0 && !a.slot_delta) {
-                double *bp = a.bc + (a.ext ? a.ext[v] : v);
-                __stcg(bp, __ldcg(bp) + add);
+                // one add per vertex per sweep (one warp finishes a vertex), and
+                // sweeps are ordered by the grid barrier: the adds reach bc[v]
+                // in sweep order, the same bits as a load-add-store, without
+                // waiting for the load
+                atomicAdd(a.bc + (a.ext ? a.ext[v] : v), add);
             }
         }
     }
