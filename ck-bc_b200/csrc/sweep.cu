@@ -55,9 +55,11 @@
 // one-vertex tile sums lane-wise over the rounds and then over the lanes in
 // a fixed butterfly; a hub's chunk totals are stored in one slot per chunk
 // and added in chunk order by the chunk that arrives last.  The segments of
-// a vertex depend on that vertex alone, and no floating-point atomics are
-// used, so a run's results are bitwise reproducible and a source's
-// contribution does not depend on the batch it shares.
+// a vertex depend on that vertex alone, and no floating-point atomic ever
+// races another (the one such add, into bc, is made once per vertex per
+// sweep, and sweeps are ordered by the grid barrier), so a run's results are
+// bitwise reproducible and a source's contribution does not depend on the
+// batch it shares.
 //
 // Child marks.  A backward sweep at level d reads every edge of every vertex
 // of level d to find its children at level d + 1.  When level d + 1 holds far

@@ -2,7 +2,8 @@
 
 Every neighbour sum is formed in a fixed order (adjacency order within a
 lane's run, lane order across a warp, round order within a tile, chunk order
-across a hub's chunks), with no floating-point atomics.  So the same run
+across a hub's chunks), with no floating-point atomics in those sums (the one
+FP64 atomic add, into bc, meets no other add in its sweep).  So the same run
 twice gives the same bits, and one source's dependencies do not depend on
 which other sources share its batch or which slot it sits in."""
 import numpy as np
