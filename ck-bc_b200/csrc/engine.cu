@@ -677,7 +677,7 @@ static int graph_create_impl(const uint32_t *offsets, const uint32_t *adj, uint3
     g->nnz = nnz;
     g->flags = flags;
     if (const char *e = getenv("BCG_PUSH_PULL_RATIO")) g->ratio = (float)atof(e);
-    if (const char *e = getenv("BCG_CHILD_MARK_RATIO")) g->mark_ratio = (uint32_t)atoi(e);
+    if (const char *e = getenv("BCG_CHILD_MARK_RATIO")) g->mark_ratio = (uint32_t)std::min(strtoul(e, nullptr, 10), 1024ul);
     if (const char *e = getenv("BCG_TILE_SHAPE")) {  // "<vertices>x<entries>", e.g. 32x128
         unsigned tv = 0, te = 0;
         if (sscanf(e, "%ux%u", &tv, &te) == 2 && tv >= 1 && tv <= (unsigned)kTileVerts && te >= 1 &&

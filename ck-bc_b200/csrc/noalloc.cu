@@ -404,7 +404,7 @@ extern "C" int bcg_bc_noalloc(const uint32_t *d_offsets, const uint32_t *d_adj, 
     a.push_pull_ratio = 0.2f;
     if (const char *e = getenv("BCG_PUSH_PULL_RATIO")) a.push_pull_ratio = (float)atof(e);
     a.mark_ratio = 8;
-    if (const char *e = getenv("BCG_CHILD_MARK_RATIO")) a.mark_ratio = (uint32_t)atoi(e);
+    if (const char *e = getenv("BCG_CHILD_MARK_RATIO")) a.mark_ratio = (uint32_t)std::min(strtoul(e, nullptr, 10), 1024ul);
     a.directed = 0;
     for (int pass = 0; pass < 2; ++pass) {
         const bool ext = pass == 1;
