@@ -123,16 +123,20 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def traffic_per_source(prune: str):
+def traffic_per_source(prune: str, kernel: str):
     """DRAM bytes per root of the sweep kernel from the committed ncu summary
-    of the same pruning mode (profiles/sweep_traffic.json), else None."""
+    of the same pruning mode (profiles/sweep_traffic.json), if it was captured
+    from the same kernel instantiation; else None and the reason."""
     p = os.path.join(ROOT, "profiles", "sweep_traffic.json")
     try:
         with open(p) as f:
             d = json.load(f)
-        e = d[prune] if prune in d else (d if prune == "degree1" and "dram_bytes_per_source" in d else None)
+        e = d.get(prune)
         if e is None:
             return None, ""
+        if e.get("kernel") != kernel:
+            return None, (f"no ncu capture of {kernel} in this pruning mode (the committed one is of "
+                          f"{e.get('kernel')}, an earlier build)")
         return float(e["dram_bytes_per_source"]), e.get("note", "")
     except Exception:
         return None, ""
@@ -669,7 +673,8 @@ def main():
     alg_bytes = 16.0 * edges + 56.0 * cverts + 8.0 * ran
     kern_s = sum(kern_ms) / 1e3
     achieved = alg_bytes / kern_s / 1e9
-    tps, tnote = traffic_per_source(args.prune)
+    tps, tnote = traffic_per_source(args.prune, f"bcg::bc_sweep_kernel<{int(st.batch_width)}, "
+                                                f"{'true' if st.extended_sigma else 'false'}>")
     traffic = tps * (ran / args.steps) if tps is not None else None
     # the same bytes per search over the graph the kernel actually walks (the
     # pruned graph, one search per root however many sources it stands for)
