@@ -71,3 +71,15 @@ def test_gpus_flag_starts_its_ranks():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2
     assert d["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_cpu_baseline_reports_the_pruned_leg():
+    """The bench line's cpu_baseline: the unpruned oracle on a bounded sample
+    and, on the same sources, the tree-pruned oracle (the GPU arm's
+    algorithm), each with a positive TEPS figure."""
+    offs, adj = bcg.generate(SPEC)
+    src = bcg.sample_sources(len(offs) - 1, 64, 2)
+    cb = bench.cpu_baseline(offs, adj, src, budget_s=0.5)
+    assert cb["kind"] == "port" and cb["value"] > 0 and cb["cores"] >= 1
+    pr = cb["pruned"]
+    assert pr["value"] > 0 and pr["unit"] == "TEPS" and "pendant trees folded" in pr["sample"]
