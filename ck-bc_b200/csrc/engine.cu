@@ -219,7 +219,7 @@ static uint32_t choose_width(const bcg_graph *g, uint64_t nroots) {
     if (g->forced_width) return g->forced_width;
     double budget = 64.0 * 1024 * 1024;
     if (const char *e = getenv("BCG_STATE_BUDGET_MB")) budget = atof(e) * 1024 * 1024;
-    const double nrows = g->tile_n ? g->tile_n : g->n;  // pendant-tree mode searches the kept vertices only
+    const double nrows = g->tile_n ? g->tile_n : g->n;  // a pruned graph searches the kept vertices only
     // low-degree graphs (mean degree below 6: grids, meshes, long chains) have
     // small frontiers and many levels, so sweeps cost barriers, not gathers,
     // and the widest batch wins whether or not the rows fit L2 (measured on a
