@@ -518,18 +518,23 @@ __device__ __forceinline__ unsigned long long vsum(unsigned long long x, unsigne
 // extended form as a compare-and-swap retry loop; each failed attempt means
 // another thread's add went through, so the loop always ends).  Integer and
 // extended sums of exact counts do not depend on the order of the adds.
+// Returns the value before the add: 0 only for the first add to a vertex not
+// reached before (every sigma added is at least 1; a wrapped sum sets the
+// overflow flag, and the run is then redone with extended counts).
 template <bool EXT>
-__device__ __forceinline__ void sigma_atomic(unsigned long long *p, unsigned long long y, const BatchArgs &a) {
+__device__ __forceinline__ unsigned long long sigma_add_old(unsigned long long *p, unsigned long long y,
+                                                            const BatchArgs &a) {
     if (EXT) {
         unsigned long long old = *reinterpret_cast<volatile unsigned long long *>(p), seen;
         do {
             seen = old;
             old = atomicCAS(p, seen, ext_add(seen, y));
         } while (old != seen);
-    } else {
-        const unsigned long long old = atomicAdd(p, y);
-        if (old + y < y) flag_overflow(a.ctrl);
+        return seen;
     }
+    const unsigned long long old = atomicAdd(p, y);
+    if (old + y < y) flag_overflow(a.ctrl);
+    return old;
 }
 
 // One tile (or one part of a split tile), processed by one warp.  The tile's
@@ -678,19 +683,16 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
                     for (int k = 0; k < S; ++k) {
                         if (!((jm >> k) & 1u)) continue;
                         const uint16_t L = w_lvl(lw[q], k);
-                        bool take = (L == (uint16_t)(d + 1));
-                        if (L == kUnvisited) {
-                            const uint16_t old = atomicCAS(reinterpret_cast<unsigned short *>(lvl_at(wrow, k)),
-                                                           (unsigned short)kUnvisited, (unsigned short)(d + 1));
-                            if (old == kUnvisited) {
-                                lc.add(k, a.vinfo[wv]);
-                                take = true;
-                                claimed_any = true;
-                            } else {
-                                take = (old == (uint16_t)(d + 1));
-                            }
+                        // unvisited, or reached at d + 1 in this sweep: a DAG
+                        // edge either way (levels only move from unvisited to
+                        // d + 1 during a push); the add that finds sigma still
+                        // 0 is the first, and its lane claims the vertex
+                        if (L != (uint16_t)(d + 1) && L != kUnvisited) continue;
+                        if (sigma_add_old<EXT>(val_at<S>(wrow, k), ws.own[jq[q]][k], a) == 0ull) {
+                            *lvl_at(wrow, k) = (uint16_t)(d + 1);
+                            lc.add(k, a.vinfo[wv]);
+                            claimed_any = true;
                         }
-                        if (take) sigma_atomic<EXT>(val_at<S>(wrow, k), ws.own[jq[q]][k], a);
                     }
                     if (claimed_any) app = claim_tile(a, wv, x.key_next);
                 }
