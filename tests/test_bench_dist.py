@@ -83,3 +83,17 @@ def test_cpu_baseline_reports_the_pruned_leg():
     assert cb["kind"] == "port" and cb["value"] > 0 and cb["cores"] >= 1
     pr = cb["pruned"]
     assert pr["value"] > 0 and pr["unit"] == "TEPS" and "pendant trees folded" in pr["sample"]
+
+
+def test_traffic_only_from_a_capture_of_the_same_kernel():
+    """roofline.traffic comes from the committed ncu summary only when it was
+    captured from the kernel instantiation that ran; otherwise null, with the
+    reason in the note."""
+    with open(os.path.join(ROOT, "profiles", "sweep_traffic.json")) as f:
+        d = json.load(f)
+    k = d["trees"]["kernel"]
+    tps, note = bench.traffic_per_source("trees", k)
+    assert tps == d["trees"]["dram_bytes_per_source"] and note
+    tps, note = bench.traffic_per_source("trees", k.replace("false", "true"))
+    assert tps is None and "no ncu capture" in note
+    assert bench.traffic_per_source("no-such-mode", k) == (None, "")
