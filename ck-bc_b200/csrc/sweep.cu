@@ -666,7 +666,8 @@ __device__ void warp_tile(const BatchArgs &a, Smem<S> &sm, WarpSmem<S> &ws, uint
                     }
                 }
             }
-            // the targets' level blocks, then claim / add with atomics
+            // the targets' level blocks, then the sigma adds (the first add to
+            // a vertex claims it)
             LaneCounts<S> lc;
             uint32_t lw[kItems][NL];
 #pragma unroll
